@@ -1,0 +1,276 @@
+"""apo_b200 -- B200-native builder of 3D Apollonius diagrams (additively weighted Voronoi
+diagrams of spheres), a drop-in for the GPU path of the apo library (PlathC/apo).
+
+Python mirror of the reference's public interface (apo/include/apo/gpu/algorithm.hpp:9-59,
+apo/include/apo/gpu/algorithm.cuh:12-46) over the C ABI of libapo2.so (include/apo2.h):
+
+    diagram = computeApolloniusDiagram(sites)        # VertexDiagram
+    full    = computeFullApolloniusDiagram(sites)    # FullDiagram
+    algo = AlgorithmGPU(sites); algo.build(); algo.toHost(); algo.toHostFull(); algo.toTopology()
+
+`sites` is an (n, 4) array of (x, y, z, r) or a flat array of 4n values, float32 or
+float64 (the reference's FP64 `Real`). Site ids in every output are indices into it.
+
+All compute runs in the CUDA library; importing this module does not load it, and every
+call that needs it raises if it cannot be loaded (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libapo2.so")
+
+APO2_OK, APO2_ERR_INVALID_ARG, APO2_ERR_CAPACITY, APO2_ERR_ITER_LIMIT, APO2_ERR_CUDA = 0, 1, 2, 3, 4
+APO2_ERR_NOT_BUILT, APO2_ERR_OUT_OF_MEMORY, APO2_ERR_TOO_LARGE = 5, 6, 7
+APO2_F32, APO2_F64 = 0, 1
+APO2_HOST, APO2_DEVICE = 0, 1
+
+_STATUS_NAMES = {
+    0: "APO2_OK", 1: "APO2_ERR_INVALID_ARG", 2: "APO2_ERR_CAPACITY", 3: "APO2_ERR_ITER_LIMIT",
+    4: "APO2_ERR_CUDA", 5: "APO2_ERR_NOT_BUILT", 6: "APO2_ERR_OUT_OF_MEMORY", 7: "APO2_ERR_TOO_LARGE",
+}
+
+
+class Apo2Error(RuntimeError):
+    def __init__(self, status: int, text: str):
+        super().__init__(f"{_STATUS_NAMES.get(status, status)}: {text}")
+        self.status = status
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("k", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32),
+                ("device", ctypes.c_uint32), ("stage_timing", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 11)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("buried", ctypes.c_uint32), ("certified_after_knn", ctypes.c_uint32),
+                ("validation_rounds", ctypes.c_uint32), ("error_flags", ctypes.c_uint32), ("reserved0", ctypes.c_uint32),
+                ("vertex_records", ctypes.c_uint64), ("edge_records", ctypes.c_uint64),
+                ("output_vertices", ctypes.c_uint64), ("output_closed_edges", ctypes.c_uint64),
+                ("ms_bounds", ctypes.c_double), ("ms_sort", ctypes.c_double), ("ms_tree", ctypes.c_double),
+                ("ms_knn", ctypes.c_double), ("ms_cells", ctypes.c_double), ("ms_vertex_validation", ctypes.c_double),
+                ("ms_edge_validation", ctypes.c_double), ("ms_bisector_validation", ctypes.c_double),
+                ("ms_output", ctypes.c_double), ("device_bytes", ctypes.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("reserved")}
+
+
+_lib = None
+
+# Every symbol of include/apo2.h with its ctypes signature.
+_P, _U32, _U64, _I = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+SIGNATURES = {
+    "apo2_version": (ctypes.c_char_p, []),
+    "apo2_last_error_string": (ctypes.c_char_p, []),
+    "apo2_create": (_I, [_P, _U32, _I, _I, _P, _P]),
+    "apo2_set_sites": (_I, [_P, _P, _I, _I, _P]),
+    "apo2_build": (_I, [_P, _P, _I]),
+    "apo2_build_and_extract": (_I, [_P, _P]),
+    "apo2_output_counts": (_I, [_P, _P, _P]),
+    "apo2_output_device": (_I, [_P, _P, _P, _P, _P]),
+    "apo2_get_vertices": (_I, [_P, _P, _P, _U64, _I, _P]),
+    "apo2_get_closed_edges": (_I, [_P, _P, _P, _U64, _I, _P]),
+    "apo2_get_topology": (_I, [_P, _P, _U64, _P, _U64, _P, _U64, _P, _P, _P]),
+    "apo2_get_cell": (_I, [_P, _U32, _P, _U32, _P, _P, _U32, _P]),
+    "apo2_debug_array": (_I, [_P, ctypes.c_char_p, _P, _U64, _P]),
+    "apo2_get_stats": (_I, [_P, _P]),
+    "apo2_destroy": (_I, [_P]),
+    "apo2_compute_diagram": (_I, [_P, _U32, _I, _P, _P, _P]),
+    "apo2_compute_full_diagram": (_I, [_P, _U32, _I, _P, _P, _P, _P, _P, _P]),
+    "apo2_free": (None, [_P]),
+    "apo2_lbvh_scratch_bytes": (_U64, [_U32]),
+    "apo2_lbvh_build": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "apo2_radix_sort_scratch_bytes": (_U64, [_U32]),
+    "apo2_radix_sort_pairs": (_I, [_P, _P, _U32, _P, _P]),
+}
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load_library(build_if_missing: bool = True):
+    """Loads libapo2.so (building it in-tree when missing). Raises if it cannot."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise OSError(f"{LIB_PATH} is missing; run apo_b200/build.py")
+        from . import build as _build
+        _build.build()
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != APO2_OK:
+        raise Apo2Error(status, load_library().apo2_last_error_string().decode())
+
+
+def _as_sites(sites) -> tuple[np.ndarray, int]:
+    a = np.asarray(sites)
+    if a.dtype not in (np.float32, np.float64):
+        a = a.astype(np.float64)
+    a = np.ascontiguousarray(a.reshape(-1, 4))
+    return a, (APO2_F64 if a.dtype == np.float64 else APO2_F32)
+
+
+@dataclass
+class VertexDiagram:
+    """Host structure of the reference (algorithm.hpp:10-15)."""
+    vertices: np.ndarray = field(default_factory=lambda: np.zeros(0))                      # Real4 {x,y,z,w}
+    verticesId: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.uint32))   # {i,j,k,l}
+    invalidationId: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.uint32))
+
+
+@dataclass
+class FullDiagram(VertexDiagram):
+    """Host structure of the reference (algorithm.hpp:18-26)."""
+    closedEdgesId: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.uint32))  # {i,j,k,0}
+    closedEdgesMin: np.ndarray = field(default_factory=lambda: np.zeros(0))                  # Real4
+
+
+@dataclass
+class Topology:
+    """Host structure of the reference (algorithm.hpp:28-33)."""
+    quadrisectors: np.ndarray
+    trisectors: np.ndarray
+    bisectors: np.ndarray
+
+
+class AlgorithmGPU:
+    """Counterpart of `apo::gpu::AlgorithmGPU<K>` (algorithm.cuh:12-46)."""
+
+    def __init__(self, sites, k: int = 16, max_iterations: int = 10, device: int = 0, stage_timing: bool = False):
+        lib = load_library()
+        self._sites, dtype = _as_sites(sites)
+        self.n = int(self._sites.shape[0])
+        opt = Options()
+        opt.struct_size = ctypes.sizeof(Options)
+        opt.k = k
+        opt.max_iterations = max_iterations
+        opt.device = device
+        opt.stage_timing = 1 if stage_timing else 0
+        handle = ctypes.c_void_p()
+        _check(lib.apo2_create(self._sites.ctypes.data, self.n, dtype, APO2_HOST, ctypes.byref(opt), ctypes.byref(handle)))
+        self._h = handle
+        self._lib = lib
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.apo2_destroy(h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def build(self, stream: int = 0, synchronize: bool = True) -> None:
+        _check(self._lib.apo2_build(self._h, ctypes.c_void_p(stream), 1 if synchronize else 0))
+
+    def build_and_extract(self, stream: int = 0) -> None:
+        _check(self._lib.apo2_build_and_extract(self._h, ctypes.c_void_p(stream)))
+
+    def output_counts(self) -> tuple[int, int]:
+        v, c = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(self._lib.apo2_output_counts(self._h, ctypes.byref(v), ctypes.byref(c)))
+        return v.value, c.value
+
+    def _copy(self, fn, count: int):
+        pos = np.zeros((count, 4), dtype=np.float64)
+        ids = np.zeros((count, 4), dtype=np.uint32)
+        written = ctypes.c_uint64()
+        _check(fn(self._h, pos.ctypes.data, ids.ctypes.data, count, APO2_HOST, ctypes.byref(written)))
+        return pos.reshape(-1), ids.reshape(-1)
+
+    def toHost(self, validate: bool = True) -> VertexDiagram:
+        v, _ = self.output_counts()
+        pos, ids = self._copy(self._lib.apo2_get_vertices, v)
+        return VertexDiagram(vertices=pos, verticesId=ids)
+
+    def toHostFull(self, validate: bool = True) -> FullDiagram:
+        v, c = self.output_counts()
+        pos, ids = self._copy(self._lib.apo2_get_vertices, v)
+        cpos, cids = self._copy(self._lib.apo2_get_closed_edges, c)
+        return FullDiagram(vertices=pos, verticesId=ids, closedEdgesId=cids, closedEdgesMin=cpos)
+
+    def toTopology(self) -> Topology:
+        q, t, b = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(self._lib.apo2_get_topology(self._h, None, 0, None, 0, None, 0, ctypes.byref(q), ctypes.byref(t), ctypes.byref(b)))
+        qa = np.zeros(4 * q.value, dtype=np.uint32)
+        ta = np.zeros(3 * t.value, dtype=np.uint32)
+        ba = np.zeros(2 * b.value, dtype=np.uint32)
+        _check(self._lib.apo2_get_topology(self._h, qa.ctypes.data, q.value, ta.ctypes.data, t.value, ba.ctypes.data, b.value,
+                                           ctypes.byref(q), ctypes.byref(t), ctypes.byref(b)))
+        return Topology(quadrisectors=qa, trisectors=ta, bisectors=ba)
+
+    def cell(self, site: int) -> tuple[np.ndarray, np.ndarray]:
+        """Per-cell store of one input site: vertices (j, k, l, type) and edges (j, k, count)."""
+        vn, en = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(self._lib.apo2_get_cell(self._h, site, None, 0, ctypes.byref(vn), None, 0, ctypes.byref(en)))
+        v = np.zeros(4 * vn.value, dtype=np.uint32)
+        e = np.zeros(3 * en.value, dtype=np.uint32)
+        _check(self._lib.apo2_get_cell(self._h, site, v.ctypes.data, vn.value, ctypes.byref(vn), e.ctypes.data, en.value,
+                                       ctypes.byref(en)))
+        return v.reshape(-1, 4), e.reshape(-1, 3)
+
+    _DEBUG_DTYPES = {"indices": np.uint32, "parent": np.int32, "left": np.int32, "right": np.int32,
+                     "aabb": np.float32, "sizes": np.uint32, "morton": np.uint64, "sites_sorted": np.float64,
+                     "status": np.uint8, "knn": np.uint32, "known_radii": np.float32, "vertex_nb": np.uint32,
+                     "edge_nb": np.uint32, "vertices": np.uint32, "edges": np.uint32}
+
+    def debug_array(self, name: str) -> np.ndarray:
+        """Internal array by name (sorted-space ids), for parity checks."""
+        dt = self._DEBUG_DTYPES[name]
+        count = ctypes.c_uint64()
+        _check(self._lib.apo2_debug_array(self._h, name.encode(), None, 0, ctypes.byref(count)))
+        out = np.zeros(count.value, dtype=dt)
+        _check(self._lib.apo2_debug_array(self._h, name.encode(), out.ctypes.data, out.nbytes, ctypes.byref(count)))
+        return out
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(self._lib.apo2_get_stats(self._h, ctypes.byref(s)))
+        return s.as_dict()
+
+
+def computeApolloniusDiagram(sites) -> VertexDiagram:
+    """`apo::gpu::computeApolloniusDiagram` (algorithm.hpp:58, src/gpu/algorithm.cu:6-15)."""
+    lib = load_library()
+    a, dtype = _as_sites(sites)
+    pos, ids, count = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64()
+    _check(lib.apo2_compute_diagram(a.ctypes.data, a.shape[0], dtype, ctypes.byref(pos), ctypes.byref(ids), ctypes.byref(count)))
+    try:
+        n = count.value
+        p = np.ctypeslib.as_array(ctypes.cast(pos, ctypes.POINTER(ctypes.c_double)), shape=(4 * n,)).copy() if n else np.zeros(0)
+        i = np.ctypeslib.as_array(ctypes.cast(ids, ctypes.POINTER(ctypes.c_uint32)), shape=(4 * n,)).copy() if n else np.zeros(0, np.uint32)
+    finally:
+        lib.apo2_free(pos)
+        lib.apo2_free(ids)
+    return VertexDiagram(vertices=p, verticesId=i)
+
+
+def computeFullApolloniusDiagram(sites) -> FullDiagram:
+    """`apo::gpu::computeFullApolloniusDiagram` (algorithm.hpp:59, src/gpu/algorithm.cu:17-26)."""
+    algo = AlgorithmGPU(sites)
+    try:
+        algo.build()
+        return algo.toHostFull(True)
+    finally:
+        algo.close()

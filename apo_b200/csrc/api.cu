@@ -1,0 +1,805 @@
+// C ABI of the builder (include/apo2.h): handle lifetime, device memory, the build
+// sequence on one stream, output extraction and the host-side topology.
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <set>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/apo2.h"
+#include "cells.cuh"
+
+namespace
+{
+    using namespace apo2;
+
+    thread_local std::string g_last_error;
+
+    apo2_status fail( apo2_status code, const std::string & text )
+    {
+        g_last_error = text;
+        return code;
+    }
+
+    apo2_status cuda_fail( cudaError_t err, const char * where )
+    {
+        return fail( err == cudaErrorMemoryAllocation ? APO2_ERR_OUT_OF_MEMORY : APO2_ERR_CUDA,
+                     std::string( where ) + ": " + cudaGetErrorString( err ) );
+    }
+
+#define APO2_CUDA( call, where )                 \
+    do                                           \
+    {                                            \
+        const cudaError_t e_ = ( call );         \
+        if ( e_ != cudaSuccess )                 \
+            return cuda_fail( e_, where );       \
+    } while ( 0 )
+
+    size_t align256( size_t b ) { return ( b + 255 ) & ~size_t( 255 ); }
+
+    // One device allocation carved into the build's arrays.
+    struct Arena
+    {
+        char * base = nullptr;
+        size_t size = 0, used = 0;
+        template<class T>
+        T * take( size_t count )
+        {
+            T * p = reinterpret_cast<T *>( base + used );
+            used += align256( sizeof( T ) * count );
+            return p;
+        }
+    };
+
+    constexpr int kStages = 10;
+} // namespace
+
+struct apo2_handle
+{
+    uint32_t     n = 0;
+    apo2_options options {};
+    int          device = 0;
+
+    Arena          arena;
+    void *         input     = nullptr; // caller sites (device copy)
+    bool           input_f64 = false;
+    double4 *      input_d4  = nullptr; // float64 copy in input order
+    BoundsPartial * partials = nullptr;
+    uint32_t       partial_count = 0;
+    uint32_t *     bounds_counter = nullptr;
+    Scene *        scene          = nullptr;
+    Tree           tree;
+    SortScratch    sort;
+    CellContext    cells;
+    uint32_t *     tasks       = nullptr;
+    uint32_t *     task_counts = nullptr; // one per validation round
+    uint32_t *     error       = nullptr;
+
+    OutputBuffers out;
+    void *        out_alloc = nullptr;
+    bool          built     = false;
+    bool          extracted = false;
+
+    cudaEvent_t events[ kStages + 1 ] = {};
+    bool        timing                = false;
+    apo2_stats  stats {};
+};
+
+namespace
+{
+    apo2_status ensure_output_capacity( apo2_handle * h, uint64_t vcap, uint64_t ccap )
+    {
+        if ( h->out_alloc && vcap <= h->out.vcap && ccap <= h->out.ccap )
+            return APO2_OK;
+        if ( h->out_alloc )
+            cudaFree( h->out_alloc );
+        h->out_alloc        = nullptr;
+        const size_t bytes  = align256( sizeof( double4 ) * vcap ) + align256( sizeof( uint4 ) * vcap )
+                             + align256( sizeof( double4 ) * ccap ) + align256( sizeof( uint4 ) * ccap );
+        APO2_CUDA( cudaMalloc( &h->out_alloc, bytes ), "output allocation" );
+        char * p    = static_cast<char *>( h->out_alloc );
+        h->out.vpos = reinterpret_cast<double4 *>( p );
+        p += align256( sizeof( double4 ) * vcap );
+        h->out.vids = reinterpret_cast<uint4 *>( p );
+        p += align256( sizeof( uint4 ) * vcap );
+        h->out.cpos = reinterpret_cast<double4 *>( p );
+        p += align256( sizeof( double4 ) * ccap );
+        h->out.cids = reinterpret_cast<uint4 *>( p );
+        h->out.vcap = vcap;
+        h->out.ccap = ccap;
+        return APO2_OK;
+    }
+
+    apo2_status upload_sites( apo2_handle * h, const void * sites, apo2_dtype dtype, apo2_location location, cudaStream_t s )
+    {
+        const size_t bytes = size_t( h->n ) * ( dtype == APO2_F64 ? 32 : 16 );
+        if ( ( dtype == APO2_F64 ) != h->input_f64 )
+            return fail( APO2_ERR_INVALID_ARG, "dtype differs from the handle's" );
+        APO2_CUDA( cudaMemcpyAsync( h->input, sites, bytes, location == APO2_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s ),
+                   "site upload" );
+        h->built     = false;
+        h->extracted = false;
+        return APO2_OK;
+    }
+
+    void record( apo2_handle * h, int stage, cudaStream_t s )
+    {
+        if ( h->timing )
+            cudaEventRecord( h->events[ stage ], s );
+    }
+
+    apo2_status enqueue_build( apo2_handle * h, cudaStream_t s )
+    {
+        const uint32_t n = h->n;
+        record( h, 0, s );
+        cudaMemsetAsync( h->error, 0, sizeof( uint32_t ), s );
+        launch_bounds( h->input, h->input_f64, n, h->input_d4, h->partials, h->partial_count, h->bounds_counter, h->scene,
+                       h->tree.sites + n, s );
+        record( h, 1, s );
+        launch_tree( h->tree, n, h->input_d4, h->scene, h->sort, s );
+        record( h, 2, s ); // bounds+Morton+sort+tree recorded as one span plus the sort below
+        launch_knn( h->cells, s );
+        record( h, 3, s );
+        launch_cells( h->cells, s );
+        record( h, 4, s );
+        const uint32_t rounds = h->options.max_iterations;
+        for ( uint32_t r = 0; r < rounds; r++ )
+        {
+            launch_tasks( h->cells, h->tasks, h->task_counts + r, s );
+            launch_vertex_validation( h->cells, h->tasks, h->task_counts + r, s );
+            launch_edge_validation( h->cells, h->tasks, h->task_counts + r, s );
+        }
+        record( h, 5, s );
+        launch_bisector_validation( h->cells, s );
+        record( h, 6, s );
+        const cudaError_t err = cudaGetLastError();
+        if ( err != cudaSuccess )
+            return cuda_fail( err, "build launch" );
+        h->built     = true;
+        h->extracted = false;
+        return APO2_OK;
+    }
+
+    apo2_status enqueue_extract( apo2_handle * h, cudaStream_t s )
+    {
+        launch_output( h->cells, h->out, s );
+        record( h, 7, s );
+        const cudaError_t err = cudaGetLastError();
+        if ( err != cudaSuccess )
+            return cuda_fail( err, "output launch" );
+        h->extracted = true;
+        return APO2_OK;
+    }
+
+    apo2_status finish( apo2_handle * h, cudaStream_t s )
+    {
+        APO2_CUDA( cudaStreamSynchronize( s ), "build" );
+        uint32_t err = 0;
+        APO2_CUDA( cudaMemcpy( &err, h->error, sizeof( uint32_t ), cudaMemcpyDeviceToHost ), "error word" );
+        h->stats.error_flags = err;
+        if ( err )
+            return fail( APO2_ERR_CAPACITY, "capacity flags " + std::to_string( err ) );
+        return APO2_OK;
+    }
+
+    // Makes sure the output arrays hold everything the last extraction counted (one
+    // synchronisation; a re-extraction only when the capacity had to grow).
+    apo2_status settle_output( apo2_handle * h, cudaStream_t s )
+    {
+        if ( !h->built )
+            return fail( APO2_ERR_NOT_BUILT, "no build yet" );
+        if ( !h->extracted )
+        {
+            apo2_status st = enqueue_extract( h, s );
+            if ( st != APO2_OK )
+                return st;
+        }
+        APO2_CUDA( cudaStreamSynchronize( s ), "extract" );
+        uint64_t totals[ 2 ];
+        APO2_CUDA( cudaMemcpy( totals, h->out.totals, sizeof( totals ), cudaMemcpyDeviceToHost ), "output totals" );
+        if ( totals[ 0 ] > h->out.vcap || totals[ 1 ] > h->out.ccap )
+        {
+            apo2_status st = ensure_output_capacity( h, totals[ 0 ] + totals[ 0 ] / 8 + 1024, totals[ 1 ] + totals[ 1 ] / 8 + 1024 );
+            if ( st != APO2_OK )
+                return st;
+            st = enqueue_extract( h, s );
+            if ( st != APO2_OK )
+                return st;
+            APO2_CUDA( cudaStreamSynchronize( s ), "extract" );
+        }
+        h->stats.output_vertices     = totals[ 0 ];
+        h->stats.output_closed_edges = totals[ 1 ];
+        return APO2_OK;
+    }
+
+    template<class T>
+    std::vector<T> download( const T * p, size_t count )
+    {
+        std::vector<T> v( count );
+        if ( count )
+            cudaMemcpy( v.data(), p, sizeof( T ) * count, cudaMemcpyDeviceToHost );
+        return v;
+    }
+} // namespace
+
+extern "C" {
+
+const char * apo2_version( void ) { return "apo2 1.0 (sm_100a)"; }
+
+const char * apo2_last_error_string( void ) { return g_last_error.c_str(); }
+
+apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_location location, const apo2_options * options,
+                         apo2_handle ** out )
+{
+    if ( !out || !sites || n < 2 || ( dtype != APO2_F32 && dtype != APO2_F64 )
+         || ( location != APO2_HOST && location != APO2_DEVICE ) )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_create" );
+    if ( n > ( 1u << 28 ) )
+        return fail( APO2_ERR_TOO_LARGE, "at most 2^28 sites" );
+    apo2_options opt {};
+    if ( options )
+    {
+        if ( options->struct_size != sizeof( apo2_options ) )
+            return fail( APO2_ERR_INVALID_ARG, "apo2_options.struct_size mismatch" );
+        opt = *options;
+    }
+    if ( opt.k == 0 )
+        opt.k = 16;
+    if ( opt.k > kMaxK )
+        return fail( APO2_ERR_INVALID_ARG, "k is at most 16" );
+    if ( opt.max_iterations == 0 )
+        opt.max_iterations = 10;
+    opt.max_iterations = std::min( opt.max_iterations, 64u );
+
+    APO2_CUDA( cudaSetDevice( int( opt.device ) ), "cudaSetDevice" );
+    apo2_handle * h = new ( std::nothrow ) apo2_handle {};
+    if ( !h )
+        return fail( APO2_ERR_OUT_OF_MEMORY, "host allocation" );
+    h->n         = n;
+    h->options   = opt;
+    h->device    = int( opt.device );
+    h->input_f64 = dtype == APO2_F64;
+    configure_cell_kernels();
+
+    // sizes
+    const size_t nodes = 2 * size_t( n ) - 1;
+    h->partial_count   = 148 * 4;
+    const size_t sortBytes = sort_scratch_bytes( n );
+    const size_t scanWords = output_scan_scratch_words( n );
+    size_t       total     = 0;
+    total += align256( size_t( n ) * ( h->input_f64 ? 32 : 16 ) );
+    total += align256( sizeof( double4 ) * n );
+    total += align256( bounds_partial_bytes( h->partial_count ) ) + align256( 4 ) + align256( sizeof( Scene ) );
+    total += align256( 8 * size_t( n ) ) + align256( 4 * size_t( n ) ) + align256( sizeof( double4 ) * ( n + kArtificial ) )
+             + align256( sizeof( float4 ) * n ) + 3 * align256( 4 * nodes ) + align256( sizeof( float4 ) * 2 * nodes )
+             + align256( 4 * nodes ) + align256( 4 * size_t( n ) ) + align256( sizeof( WideNode ) * n );
+    total += align256( sortBytes );
+    total += align256( size_t( n ) ) + align256( 4 * size_t( n ) * opt.k ) + align256( 4 * size_t( n ) ) * 3
+             + align256( sizeof( uint4 ) * kMaxVertices * size_t( n ) ) + align256( sizeof( uint4 ) * kMaxEdges * size_t( n ) );
+    total += align256( 4 * size_t( n ) ) + align256( 4 * 64 ) + align256( 4 );
+    total += align256( 4 * size_t( n ) ) * 2 + align256( 4 * scanWords * 2 ) + align256( 16 );
+    h->arena.size = total;
+    cudaError_t err = cudaMalloc( reinterpret_cast<void **>( &h->arena.base ), total );
+    if ( err != cudaSuccess )
+    {
+        delete h;
+        return cuda_fail( err, "device allocation" );
+    }
+    Arena & a         = h->arena;
+    h->input          = a.take<char>( size_t( n ) * ( h->input_f64 ? 32 : 16 ) );
+    h->input_d4       = a.take<double4>( n );
+    h->partials       = reinterpret_cast<BoundsPartial *>( a.take<char>( bounds_partial_bytes( h->partial_count ) ) );
+    h->bounds_counter = a.take<uint32_t>( 1 );
+    h->scene          = a.take<Scene>( 1 );
+    Tree & t          = h->tree;
+    t.codes           = a.take<uint64_t>( n );
+    t.indices         = a.take<uint32_t>( n );
+    t.sites           = a.take<double4>( n + kArtificial );
+    t.sites_f         = a.take<float4>( n );
+    t.parent          = a.take<int32_t>( nodes );
+    t.left            = a.take<int32_t>( nodes );
+    t.right           = a.take<int32_t>( nodes );
+    t.boxes           = a.take<float4>( 2 * nodes );
+    t.sizes           = a.take<uint32_t>( nodes );
+    t.arrivals        = a.take<uint32_t>( n );
+    t.nodes           = a.take<WideNode>( n );
+    void * sortBase   = a.take<char>( sortBytes );
+    CellContext & c   = h->cells;
+    c.n               = n;
+    c.k               = opt.k;
+    c.sites           = t.sites;
+    c.sites_f         = t.sites_f;
+    c.nodes           = t.nodes;
+    c.indices         = t.indices;
+    c.status          = a.take<uint8_t>( n );
+    c.knn             = a.take<uint32_t>( size_t( n ) * opt.k );
+    c.known_radii     = a.take<float>( n );
+    c.vertex_nb       = a.take<uint32_t>( n );
+    c.edge_nb         = a.take<uint32_t>( n );
+    c.vertices        = a.take<uint4>( size_t( n ) * kMaxVertices );
+    c.edges           = a.take<uint4>( size_t( n ) * kMaxEdges );
+    h->tasks          = a.take<uint32_t>( n );
+    h->task_counts    = a.take<uint32_t>( 64 );
+    h->error          = a.take<uint32_t>( 1 );
+    c.error           = h->error;
+    h->out.vcount     = a.take<uint32_t>( n );
+    h->out.ccount     = a.take<uint32_t>( n );
+    h->out.tile_sums  = a.take<uint32_t>( scanWords * 2 );
+    h->out.totals     = a.take<uint64_t>( 2 );
+    sort_scratch_carve( h->sort, sortBase, n, h->error );
+    if ( a.used > a.size )
+    {
+        cudaFree( a.base );
+        delete h;
+        return fail( APO2_ERR_CUDA, "arena accounting" );
+    }
+    cudaMemset( h->bounds_counter, 0, sizeof( uint32_t ) );
+    cudaMemset( h->error, 0, sizeof( uint32_t ) );
+    cudaMemset( h->out.totals, 0, 2 * sizeof( uint64_t ) );
+
+    apo2_status st = ensure_output_capacity( h, 8 * uint64_t( n ) + 1024, uint64_t( n ) / 16 + 1024 );
+    if ( st == APO2_OK )
+    {
+        h->timing = opt.stage_timing != 0;
+        if ( h->timing )
+            for ( auto & e : h->events )
+                cudaEventCreate( &e );
+        st = upload_sites( h, sites, dtype, location, 0 );
+    }
+    if ( st == APO2_OK )
+    {
+        err = cudaStreamSynchronize( 0 );
+        if ( err != cudaSuccess )
+            st = cuda_fail( err, "site upload" );
+    }
+    if ( st != APO2_OK )
+    {
+        apo2_destroy( h );
+        return st;
+    }
+    h->stats.n            = n;
+    h->stats.device_bytes = total + align256( sizeof( double4 ) * h->out.vcap ) * 2;
+    *out                  = h;
+    return APO2_OK;
+}
+
+apo2_status apo2_set_sites( apo2_handle * h, const void * sites, apo2_dtype dtype, apo2_location location, void * stream )
+{
+    if ( !h || !sites )
+        return fail( APO2_ERR_INVALID_ARG, "null argument" );
+    return upload_sites( h, sites, dtype, location, static_cast<cudaStream_t>( stream ) );
+}
+
+apo2_status apo2_build( apo2_handle * h, void * stream, int synchronize )
+{
+    if ( !h )
+        return fail( APO2_ERR_INVALID_ARG, "null handle" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    cudaStream_t s  = static_cast<cudaStream_t>( stream );
+    apo2_status  st = enqueue_build( h, s );
+    if ( st != APO2_OK || !synchronize )
+        return st;
+    return finish( h, s );
+}
+
+apo2_status apo2_build_and_extract( apo2_handle * h, void * stream )
+{
+    if ( !h )
+        return fail( APO2_ERR_INVALID_ARG, "null handle" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    cudaStream_t s  = static_cast<cudaStream_t>( stream );
+    apo2_status  st = enqueue_build( h, s );
+    if ( st != APO2_OK )
+        return st;
+    return enqueue_extract( h, s );
+}
+
+apo2_status apo2_output_counts( apo2_handle * h, uint64_t * vertices, uint64_t * closed )
+{
+    if ( !h )
+        return fail( APO2_ERR_INVALID_ARG, "null handle" );
+    apo2_status st = settle_output( h, 0 );
+    if ( st != APO2_OK )
+        return st;
+    if ( vertices )
+        *vertices = h->stats.output_vertices;
+    if ( closed )
+        *closed = h->stats.output_closed_edges;
+    return APO2_OK;
+}
+
+apo2_status apo2_output_device( apo2_handle * h, const double ** vp, const uint32_t ** vi, const double ** cp, const uint32_t ** ci )
+{
+    if ( !h )
+        return fail( APO2_ERR_INVALID_ARG, "null handle" );
+    if ( !h->extracted )
+        return fail( APO2_ERR_NOT_BUILT, "no extraction yet" );
+    if ( vp )
+        *vp = reinterpret_cast<const double *>( h->out.vpos );
+    if ( vi )
+        *vi = reinterpret_cast<const uint32_t *>( h->out.vids );
+    if ( cp )
+        *cp = reinterpret_cast<const double *>( h->out.cpos );
+    if ( ci )
+        *ci = reinterpret_cast<const uint32_t *>( h->out.cids );
+    return APO2_OK;
+}
+
+static apo2_status copy_output( apo2_handle * h, bool closed, double * pos, uint32_t * ids, uint64_t capacity,
+                                apo2_location location, uint64_t * written )
+{
+    if ( !h )
+        return fail( APO2_ERR_INVALID_ARG, "null handle" );
+    apo2_status st = settle_output( h, 0 );
+    if ( st != APO2_OK )
+        return st;
+    const uint64_t count = closed ? h->stats.output_closed_edges : h->stats.output_vertices;
+    if ( written )
+        *written = count;
+    if ( !pos && !ids )
+        return APO2_OK;
+    if ( capacity < count )
+        return fail( APO2_ERR_INVALID_ARG, "output capacity too small" );
+    const cudaMemcpyKind kind = location == APO2_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if ( pos )
+        APO2_CUDA( cudaMemcpy( pos, closed ? h->out.cpos : h->out.vpos, sizeof( double4 ) * count, kind ), "output copy" );
+    if ( ids )
+        APO2_CUDA( cudaMemcpy( ids, closed ? h->out.cids : h->out.vids, sizeof( uint4 ) * count, kind ), "output copy" );
+    return APO2_OK;
+}
+
+apo2_status apo2_get_vertices( apo2_handle * h, double * positions, uint32_t * ids, uint64_t capacity, apo2_location location,
+                               uint64_t * written )
+{
+    return copy_output( h, false, positions, ids, capacity, location, written );
+}
+
+apo2_status apo2_get_closed_edges( apo2_handle * h, double * positions, uint32_t * ids, uint64_t capacity,
+                                   apo2_location location, uint64_t * written )
+{
+    return copy_output( h, true, positions, ids, capacity, location, written );
+}
+
+apo2_status apo2_get_topology( apo2_handle * h, uint32_t * quad, uint64_t quad_cap, uint32_t * tri, uint64_t tri_cap,
+                               uint32_t * bi, uint64_t bi_cap, uint64_t * quad_count, uint64_t * tri_count, uint64_t * bi_count )
+{
+    if ( !h )
+        return fail( APO2_ERR_INVALID_ARG, "null handle" );
+    if ( !h->built )
+        return fail( APO2_ERR_NOT_BUILT, "no build yet" );
+    APO2_CUDA( cudaDeviceSynchronize(), "topology" );
+    const uint32_t n        = h->n;
+    const auto     vnb      = download( h->cells.vertex_nb, n );
+    const auto     enb      = download( h->cells.edge_nb, n );
+    const auto     vertices = download( h->cells.vertices, size_t( n ) * kMaxVertices );
+    const auto     edges    = download( h->cells.edges, size_t( n ) * kMaxEdges );
+    const auto     ix       = download( h->tree.indices, n );
+    std::vector<uint32_t> q, t, b;
+    // per sorted cell: unique tuples with the cell's id smallest (algorithm.inl:1732-1821)
+    std::vector<std::pair<uint32_t, uint32_t>> bis;
+    std::vector<std::tuple<uint32_t, uint32_t>> tris;
+    std::vector<std::tuple<uint32_t, uint32_t, uint32_t>> quads;
+    for ( uint32_t i = 0; i < n; i++ )
+    {
+        bis.clear();
+        tris.clear();
+        quads.clear();
+        for ( uint32_t e = 0; e < std::min( enb[ i ], kMaxEdges ); e++ )
+        {
+            const uint4 r = edges[ size_t( i ) * kMaxEdges + e ];
+            if ( i < r.x && r.x < n )
+                bis.emplace_back( i, r.x );
+            if ( i < r.y && r.y < n )
+                bis.emplace_back( i, r.y );
+            if ( i < r.x && i < r.y && r.x < n && r.y < n )
+                tris.emplace_back( r.x, r.y );
+        }
+        for ( uint32_t v = 0; v < std::min( vnb[ i ], kMaxVertices ); v++ )
+        {
+            const uint4 r = vertices[ size_t( i ) * kMaxVertices + v ];
+            if ( i < r.x && i < r.y && i < r.z && r.x < n && r.y < n && r.z < n )
+                quads.emplace_back( r.x, r.y, r.z );
+        }
+        std::sort( bis.begin(), bis.end() );
+        bis.erase( std::unique( bis.begin(), bis.end() ), bis.end() );
+        std::sort( tris.begin(), tris.end() );
+        tris.erase( std::unique( tris.begin(), tris.end() ), tris.end() );
+        std::sort( quads.begin(), quads.end() );
+        quads.erase( std::unique( quads.begin(), quads.end() ), quads.end() );
+        for ( auto & x : bis )
+            b.insert( b.end(), { ix[ x.first ], ix[ x.second ] } );
+        for ( auto & x : tris )
+            t.insert( t.end(), { ix[ i ], ix[ std::get<0>( x ) ], ix[ std::get<1>( x ) ] } );
+        for ( auto & x : quads )
+            q.insert( q.end(), { ix[ i ], ix[ std::get<0>( x ) ], ix[ std::get<1>( x ) ], ix[ std::get<2>( x ) ] } );
+    }
+    if ( quad_count )
+        *quad_count = q.size() / 4;
+    if ( tri_count )
+        *tri_count = t.size() / 3;
+    if ( bi_count )
+        *bi_count = b.size() / 2;
+    if ( ( quad && quad_cap < q.size() / 4 ) || ( tri && tri_cap < t.size() / 3 ) || ( bi && bi_cap < b.size() / 2 ) )
+        return fail( APO2_ERR_INVALID_ARG, "topology capacity too small" );
+    if ( quad )
+        std::memcpy( quad, q.data(), q.size() * 4 );
+    if ( tri )
+        std::memcpy( tri, t.data(), t.size() * 4 );
+    if ( bi )
+        std::memcpy( bi, b.data(), b.size() * 4 );
+    return APO2_OK;
+}
+
+apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, uint32_t vcap, uint32_t * vcount,
+                           uint32_t * edges, uint32_t ecap, uint32_t * ecount )
+{
+    if ( !h || site >= h->n )
+        return fail( APO2_ERR_INVALID_ARG, "invalid site" );
+    if ( !h->built )
+        return fail( APO2_ERR_NOT_BUILT, "no build yet" );
+    APO2_CUDA( cudaDeviceSynchronize(), "cell" );
+    const auto ix = download( h->tree.indices, h->n );
+    uint32_t   sorted = 0;
+    while ( sorted < h->n && ix[ sorted ] != site )
+        sorted++;
+    uint32_t vn = 0, en = 0;
+    cudaMemcpy( &vn, h->cells.vertex_nb + sorted, 4, cudaMemcpyDeviceToHost );
+    cudaMemcpy( &en, h->cells.edge_nb + sorted, 4, cudaMemcpyDeviceToHost );
+    vn            = std::min( vn, kMaxVertices );
+    en            = std::min( en, kMaxEdges );
+    const auto vr = download( h->cells.vertices + size_t( sorted ) * kMaxVertices, vn );
+    const auto er = download( h->cells.edges + size_t( sorted ) * kMaxEdges, en );
+    auto       map = [ & ]( uint32_t id ) { return id < h->n ? ix[ id ] : id; };
+    if ( vcount )
+        *vcount = vn;
+    if ( ecount )
+        *ecount = en;
+    if ( vertices )
+        for ( uint32_t v = 0; v < std::min( vn, vcap ); v++ )
+        {
+            vertices[ 4 * v + 0 ] = map( vr[ v ].x );
+            vertices[ 4 * v + 1 ] = map( vr[ v ].y );
+            vertices[ 4 * v + 2 ] = map( vr[ v ].z );
+            vertices[ 4 * v + 3 ] = vr[ v ].w & 0xffu;
+        }
+    if ( edges )
+        for ( uint32_t e = 0; e < std::min( en, ecap ); e++ )
+        {
+            edges[ 3 * e + 0 ] = map( er[ e ].x );
+            edges[ 3 * e + 1 ] = map( er[ e ].y );
+            edges[ 3 * e + 2 ] = er[ e ].z;
+        }
+    return APO2_OK;
+}
+
+apo2_status apo2_debug_array( apo2_handle * h, const char * name, void * dst, uint64_t capacity_bytes, uint64_t * count )
+{
+    if ( !h || !name )
+        return fail( APO2_ERR_INVALID_ARG, "null argument" );
+    APO2_CUDA( cudaDeviceSynchronize(), "debug array" );
+    const uint32_t    n     = h->n;
+    const uint64_t    nodes = 2 * uint64_t( n ) - 1;
+    const std::string key( name );
+    const void *      src   = nullptr;
+    uint64_t          elems = 0, esize = 4;
+    std::vector<uint32_t> packed;
+    if ( key == "indices" )
+        src = h->tree.indices, elems = n;
+    else if ( key == "parent" )
+        src = h->tree.parent, elems = nodes;
+    else if ( key == "left" )
+        src = h->tree.left, elems = nodes;
+    else if ( key == "right" )
+        src = h->tree.right, elems = nodes;
+    else if ( key == "aabb" )
+        src = h->tree.boxes, elems = nodes * 8;
+    else if ( key == "sizes" )
+        src = h->tree.sizes, elems = nodes;
+    else if ( key == "morton" )
+        src = h->tree.codes, elems = n, esize = 8;
+    else if ( key == "sites_sorted" )
+        src = h->tree.sites, elems = 4 * ( uint64_t( n ) + kArtificial ), esize = 8;
+    else if ( key == "status" )
+        src = h->cells.status, elems = n, esize = 1;
+    else if ( key == "knn" )
+        src = h->cells.knn, elems = uint64_t( n ) * h->cells.k;
+    else if ( key == "known_radii" )
+        src = h->cells.known_radii, elems = n;
+    else if ( key == "vertex_nb" )
+        src = h->cells.vertex_nb, elems = n;
+    else if ( key == "edge_nb" )
+        src = h->cells.edge_nb, elems = n;
+    else if ( key == "vertices" || key == "edges" )
+    {
+        const bool  isV  = key == "vertices";
+        const auto  nb   = download( isV ? h->cells.vertex_nb : h->cells.edge_nb, n );
+        const uint32_t cap = isV ? kMaxVertices : kMaxEdges;
+        const auto  all  = download( isV ? h->cells.vertices : h->cells.edges, size_t( n ) * cap );
+        for ( uint32_t i = 0; i < n; i++ )
+            for ( uint32_t r = 0; r < std::min( nb[ i ], cap ); r++ )
+            {
+                const uint4 x = all[ size_t( i ) * cap + r ];
+                packed.insert( packed.end(), { x.x, x.y, x.z, x.w } );
+            }
+        elems = packed.size();
+    }
+    else
+        return fail( APO2_ERR_INVALID_ARG, "unknown array " + key );
+    if ( count )
+        *count = elems;
+    if ( !dst )
+        return APO2_OK;
+    if ( capacity_bytes < elems * esize )
+        return fail( APO2_ERR_INVALID_ARG, "capacity too small" );
+    if ( !packed.empty() )
+        std::memcpy( dst, packed.data(), elems * esize );
+    else if ( elems )
+        APO2_CUDA( cudaMemcpy( dst, src, elems * esize, cudaMemcpyDeviceToHost ), "debug copy" );
+    return APO2_OK;
+}
+
+apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
+{
+    if ( !h || !stats )
+        return fail( APO2_ERR_INVALID_ARG, "null argument" );
+    APO2_CUDA( cudaDeviceSynchronize(), "stats" );
+    const uint32_t n = h->n;
+    const auto     status = download( h->cells.status, n );
+    const auto     vnb    = download( h->cells.vertex_nb, n );
+    const auto     enb    = download( h->cells.edge_nb, n );
+    uint32_t       err    = 0;
+    cudaMemcpy( &err, h->error, 4, cudaMemcpyDeviceToHost );
+    uint32_t counts[ 64 ] = {};
+    cudaMemcpy( counts, h->task_counts, 4 * h->options.max_iterations, cudaMemcpyDeviceToHost );
+    apo2_stats s = h->stats;
+    s.n          = n;
+    s.buried = 0;
+    s.vertex_records = 0;
+    s.edge_records   = 0;
+    for ( uint32_t i = 0; i < n; i++ )
+    {
+        s.buried += status[ i ] == kBuried;
+        s.vertex_records += vnb[ i ];
+        s.edge_records += enb[ i ];
+    }
+    s.certified_after_knn = n - s.buried - counts[ 0 ];
+    s.validation_rounds   = 0;
+    for ( uint32_t r = 0; r < h->options.max_iterations; r++ )
+        s.validation_rounds += counts[ r ] != 0;
+    s.error_flags = err;
+    if ( h->timing )
+    {
+        float ms[ kStages ] = {};
+        for ( int e = 0; e < 7; e++ )
+            cudaEventElapsedTime( &ms[ e ], h->events[ e ], h->events[ e + 1 ] );
+        s.ms_bounds              = ms[ 0 ];
+        s.ms_tree                = ms[ 1 ];
+        s.ms_knn                 = ms[ 2 ];
+        s.ms_cells               = ms[ 3 ];
+        s.ms_vertex_validation   = ms[ 4 ]; // vertex and edge rounds together
+        s.ms_bisector_validation = ms[ 5 ];
+        s.ms_output              = h->extracted ? ms[ 6 ] : 0.0;
+    }
+    *stats = s;
+    return APO2_OK;
+}
+
+apo2_status apo2_destroy( apo2_handle * h )
+{
+    if ( !h )
+        return APO2_OK;
+    cudaSetDevice( h->device );
+    cudaDeviceSynchronize();
+    if ( h->out_alloc )
+        cudaFree( h->out_alloc );
+    if ( h->arena.base )
+        cudaFree( h->arena.base );
+    if ( h->timing )
+        for ( auto & e : h->events )
+            if ( e )
+                cudaEventDestroy( e );
+    delete h;
+    return APO2_OK;
+}
+
+static apo2_status compute( const void * sites, uint32_t n, apo2_dtype dtype, double ** positions, uint32_t ** ids,
+                            uint64_t * count, double ** cpos, uint32_t ** cids, uint64_t * ccount )
+{
+    apo2_handle * h  = nullptr;
+    apo2_status   st = apo2_create( sites, n, dtype, APO2_HOST, nullptr, &h );
+    if ( st != APO2_OK )
+        return st;
+    st = apo2_build_and_extract( h, nullptr );
+    if ( st == APO2_OK )
+        st = finish( h, 0 );
+    uint64_t vc = 0, cc = 0;
+    if ( st == APO2_OK )
+        st = apo2_output_counts( h, &vc, &cc );
+    if ( st == APO2_OK )
+    {
+        *positions = static_cast<double *>( std::malloc( sizeof( double ) * 4 * std::max<uint64_t>( vc, 1 ) ) );
+        *ids       = static_cast<uint32_t *>( std::malloc( sizeof( uint32_t ) * 4 * std::max<uint64_t>( vc, 1 ) ) );
+        st         = apo2_get_vertices( h, *positions, *ids, vc, APO2_HOST, count );
+    }
+    if ( st == APO2_OK && cpos )
+    {
+        *cpos = static_cast<double *>( std::malloc( sizeof( double ) * 4 * std::max<uint64_t>( cc, 1 ) ) );
+        *cids = static_cast<uint32_t *>( std::malloc( sizeof( uint32_t ) * 4 * std::max<uint64_t>( cc, 1 ) ) );
+        st    = apo2_get_closed_edges( h, *cpos, *cids, cc, APO2_HOST, ccount );
+    }
+    apo2_destroy( h );
+    return st;
+}
+
+apo2_status apo2_compute_diagram( const void * sites, uint32_t n, apo2_dtype dtype, double ** positions, uint32_t ** ids,
+                                  uint64_t * count )
+{
+    if ( !positions || !ids || !count )
+        return fail( APO2_ERR_INVALID_ARG, "null output" );
+    return compute( sites, n, dtype, positions, ids, count, nullptr, nullptr, nullptr );
+}
+
+apo2_status apo2_compute_full_diagram( const void * sites, uint32_t n, apo2_dtype dtype, double ** positions, uint32_t ** ids,
+                                       uint64_t * count, double ** cpos, uint32_t ** cids, uint64_t * ccount )
+{
+    if ( !positions || !ids || !count || !cpos || !cids || !ccount )
+        return fail( APO2_ERR_INVALID_ARG, "null output" );
+    return compute( sites, n, dtype, positions, ids, count, cpos, cids, ccount );
+}
+
+void apo2_free( void * p ) { std::free( p ); }
+
+uint64_t apo2_lbvh_scratch_bytes( uint32_t n ) { return sort_scratch_bytes( n ) + align256( 4 * size_t( n ) ) + 256; }
+
+apo2_status apo2_lbvh_build( const float * sites, uint32_t n, const float scene_min[ 3 ], const float scene_max[ 3 ],
+                             uint32_t * indices, uint64_t * codes, int32_t * parent, int32_t * left, int32_t * right, float * aabb,
+                             uint32_t * sizes, void * scratch, void * stream )
+{
+    if ( !sites || n < 2 || !scene_min || !scene_max || !indices || !codes || !parent || !left || !right || !aabb || !scratch )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_lbvh_build" );
+    if ( n > ( 1u << 28 ) )
+        return fail( APO2_ERR_TOO_LARGE, "at most 2^28 sites" );
+    cudaStream_t s = static_cast<cudaStream_t>( stream );
+    // host float arithmetic of the reference for the scale (lbvh.cu:287-288)
+    const float3 lo    = make_float3( scene_min[ 0 ], scene_min[ 1 ], scene_min[ 2 ] );
+    const float3 scale = make_float3( 1.f / ( scene_max[ 0 ] - scene_min[ 0 ] ), 1.f / ( scene_max[ 1 ] - scene_min[ 1 ] ),
+                                      1.f / ( scene_max[ 2 ] - scene_min[ 2 ] ) );
+    char *      p        = static_cast<char *>( scratch );
+    uint32_t *  errw     = reinterpret_cast<uint32_t *>( p );
+    uint32_t *  arrivals = reinterpret_cast<uint32_t *>( p + 256 );
+    SortScratch sort;
+    sort_scratch_carve( sort, p + 256 + align256( 4 * size_t( n ) ), n, errw );
+    cudaMemsetAsync( errw, 0, 4, s );
+    launch_lbvh_f32( reinterpret_cast<const float4 *>( sites ), n, lo, scale, indices, codes, parent, left, right,
+                     reinterpret_cast<float4 *>( aabb ), sizes, arrivals, sort, s );
+    const cudaError_t err = cudaGetLastError();
+    if ( err != cudaSuccess )
+        return cuda_fail( err, "lbvh launch" );
+    return APO2_OK;
+}
+
+uint64_t apo2_radix_sort_scratch_bytes( uint32_t n ) { return sort_scratch_bytes( n ) + 256; }
+
+apo2_status apo2_radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t n, void * scratch, void * stream )
+{
+    if ( !keys || !values || !scratch )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_radix_sort_pairs" );
+    if ( n > ( 1u << 30 ) - 1 )
+        return fail( APO2_ERR_TOO_LARGE, "at most 2^30 - 1 pairs" );
+    cudaStream_t s    = static_cast<cudaStream_t>( stream );
+    uint32_t *   errw = static_cast<uint32_t *>( scratch );
+    SortScratch  sort;
+    sort_scratch_carve( sort, static_cast<char *>( scratch ) + 256, n, errw );
+    cudaMemsetAsync( errw, 0, 4, s );
+    radix_sort_pairs( keys, values, n, sort, s );
+    const cudaError_t err = cudaGetLastError();
+    if ( err != cudaSuccess )
+        return cuda_fail( err, "sort launch" );
+    return APO2_OK;
+}
+
+} // extern "C"

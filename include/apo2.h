@@ -1,0 +1,201 @@
+/*
+ * apo2 -- C ABI of the B200-native Apollonius-diagram builder.
+ *
+ * The library builds the additively weighted Voronoi (Apollonius) diagram of weighted
+ * sites (x, y, z, r) on one GPU: LBVH over the sites, kNN search, warp-per-cell cell
+ * update with the security-radius certificate, the vertex / edge / bisector validation
+ * passes, and the output extraction. Results are those of the reference apo library
+ * (PlathC/apo, FP64 `apo` target) on the same input.
+ *
+ * Conventions
+ *   - Every entry point returns an apo2_status; no C++ exception crosses this boundary.
+ *   - Pointers are plain host or device addresses; `location` says which.
+ *   - All device work of a handle runs on the stream given to apo2_build (0 = the legacy
+ *     default stream). A handle must not be used from two threads at once.
+ *   - Output site ids are indices into the caller's input array.
+ *
+ * Reference interfaces replaced (paths relative to the PlathC/apo tree):
+ *   apo/include/apo/gpu/algorithm.hpp:35-59   Algorithm, VertexDiagram, FullDiagram,
+ *                                              Topology, computeApolloniusDiagram,
+ *                                              computeFullApolloniusDiagram
+ *   apo/include/apo/gpu/algorithm.cuh:12-46   AlgorithmGPU<K>::build/toHost/toHostFull/
+ *                                              toTopology, Sample
+ *   apo/src/gpu/lbvh.cu:274-323               LBVH::build (node arrays)
+ */
+#ifndef APO2_H
+#define APO2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum apo2_status
+{
+    APO2_OK                = 0,
+    APO2_ERR_INVALID_ARG   = 1, /* null pointer, n < 2, unknown dtype / location */
+    APO2_ERR_CAPACITY      = 2, /* a per-cell store overflowed (152 vertices / 264 edges / 64 new
+                                   edges / 512 bisectors / traversal stack); results are flagged */
+    APO2_ERR_ITER_LIMIT    = 3, /* validation still had uncertified cells after the last round */
+    APO2_ERR_CUDA          = 4, /* a CUDA call failed; apo2_last_error_string has the text */
+    APO2_ERR_NOT_BUILT     = 5, /* result requested before apo2_build */
+    APO2_ERR_OUT_OF_MEMORY = 6,
+    APO2_ERR_TOO_LARGE     = 7  /* a size above a stated maximum */
+} apo2_status;
+
+typedef enum apo2_dtype
+{
+    APO2_F32 = 0, /* float  x, y, z, r */
+    APO2_F64 = 1  /* double x, y, z, r (the reference's FP64 Real) */
+} apo2_dtype;
+
+typedef enum apo2_location
+{
+    APO2_HOST   = 0,
+    APO2_DEVICE = 1
+} apo2_location;
+
+typedef struct apo2_handle apo2_handle;
+
+/* Build options. Zero-initialise, then set what differs; `struct_size` must be
+ * sizeof(apo2_options). */
+typedef struct apo2_options
+{
+    uint32_t struct_size;
+    uint32_t k;                    /* kNN neighbours per cell; 0 = 16 (reference default) */
+    uint32_t max_iterations;       /* validation rounds; 0 = 10 (algorithm.inl:1554) */
+    uint32_t device;               /* CUDA device ordinal */
+    uint32_t stage_timing;         /* 1 = record per-stage CUDA-event times (apo2_stats) */
+    uint32_t reserved[ 11 ];
+} apo2_options;
+
+/* Per-build statistics, the counterpart of AlgorithmGPU::Sample (algorithm.cuh:18-27). */
+typedef struct apo2_stats
+{
+    uint32_t n;
+    uint32_t buried;               /* cells of sites inside another site */
+    uint32_t certified_after_knn;  /* cells certified by the kNN security radius */
+    uint32_t validation_rounds;    /* vertex+edge validation rounds that had work */
+    uint32_t error_flags;          /* capacity flags (1 vertex, 2 edge, 4 new edge, 8 bisector, 16 stack) */
+    uint32_t reserved0;
+    uint64_t vertex_records;       /* sum of per-cell vertex counts */
+    uint64_t edge_records;         /* sum of per-cell edge counts */
+    uint64_t output_vertices;      /* vertices owned by their smallest site (toHost) */
+    uint64_t output_closed_edges;  /* closed trisectors owned by their smallest site */
+    double   ms_bounds;            /* bbox, Morton codes */
+    double   ms_sort;              /* onesweep radix sort */
+    double   ms_tree;              /* leaves, hierarchy, refit */
+    double   ms_knn;
+    double   ms_cells;
+    double   ms_vertex_validation;
+    double   ms_edge_validation;
+    double   ms_bisector_validation;
+    double   ms_output;
+    uint64_t device_bytes;         /* device memory held by the handle */
+} apo2_stats;
+
+/* Library version string. */
+const char * apo2_version( void );
+
+/* Text of the last error raised on this thread. */
+const char * apo2_last_error_string( void );
+
+/* Creates a handle over `n` sites. The sites are copied (or converted) to device memory
+ * immediately; the caller keeps ownership of `sites`.
+ * Replaces: AlgorithmGPU<K>::AlgorithmGPU(ConstSpan<Real>, uint32_t)
+ *           (apo/include/apo/gpu/algorithm.inl:1404-1408, src/gpu/algorithm.cpp:5-25). */
+apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_location location,
+                         const apo2_options * options, apo2_handle ** out );
+
+/* Replaces the sites of an existing handle (same n), reusing its device memory. */
+apo2_status apo2_set_sites( apo2_handle * h, const void * sites, apo2_dtype dtype, apo2_location location,
+                            void * stream );
+
+/* Builds the diagram on `stream` (a cudaStream_t; 0 = default). Asynchronous with respect to
+ * the host unless `synchronize` is non-zero, in which case the error flags are checked.
+ * Replaces: AlgorithmGPU<K>::build() (apo/include/apo/gpu/algorithm.inl:1410-1594). */
+apo2_status apo2_build( apo2_handle * h, void * stream, int synchronize );
+
+/* Builds and then extracts the output vertices / closed edges into device buffers owned by
+ * the handle (no host synchronisation); apo2_output_device returns their addresses. */
+apo2_status apo2_build_and_extract( apo2_handle * h, void * stream );
+
+/* Counts of the output (synchronises the handle's stream). */
+apo2_status apo2_output_counts( apo2_handle * h, uint64_t * vertices, uint64_t * closed_edges );
+
+/* Device addresses of the extracted output (valid until the next build or destroy):
+ * positions double4 [count], ids uint32[4*count] (original site indices i,j,k,l). */
+apo2_status apo2_output_device( apo2_handle * h, const double ** vertex_positions, const uint32_t ** vertex_ids,
+                                const double ** closed_positions, const uint32_t ** closed_ids );
+
+/* Copies the vertices owned by their smallest site (cell i < j,k,l) into caller buffers:
+ * positions (x,y,z,w) double[4*capacity], ids uint32[4*capacity] (i,j,k,l original ids).
+ * Replaces: AlgorithmGPU<K>::toHost (apo/include/apo/gpu/algorithm.inl:1596-1646). */
+apo2_status apo2_get_vertices( apo2_handle * h, double * positions, uint32_t * ids, uint64_t capacity,
+                               apo2_location location, uint64_t * written );
+
+/* Closed (vertex-free elliptic) trisectors: the trisector vertex of smaller radius and the
+ * ids (i, j, k, 0). Replaces the closed-edge half of AlgorithmGPU<K>::toHostFull
+ * (apo/include/apo/gpu/algorithm.inl:1648-1730). */
+apo2_status apo2_get_closed_edges( apo2_handle * h, double * positions, uint32_t * ids, uint64_t capacity,
+                                   apo2_location location, uint64_t * written );
+
+/* Topology as the reference's toTopology (apo/include/apo/gpu/algorithm.inl:1732-1821):
+ * per cell (sorted order) the unique bisectors (i<j), trisectors (i<j,k) and quadrisectors
+ * (i<j,k,l), mapped to original ids. Pass NULL arrays to query the counts first. */
+apo2_status apo2_get_topology( apo2_handle * h, uint32_t * quadrisectors, uint64_t quad_capacity,
+                               uint32_t * trisectors, uint64_t tri_capacity, uint32_t * bisectors,
+                               uint64_t bi_capacity, uint64_t * quad_count, uint64_t * tri_count,
+                               uint64_t * bi_count );
+
+/* Per-cell store of one site (given by original id): its vertices as (j, k, l, type) and
+ * edges as (j, k, vertex count or 0xffffffff for a closed trisector), ids original. */
+apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, uint32_t vertex_capacity,
+                           uint32_t * vertex_count, uint32_t * edges, uint32_t edge_capacity,
+                           uint32_t * edge_count );
+
+/* Raw internal arrays for parity checks, host copies. `name` is one of: "indices"
+ * (sorted -> original id, u32[n]), "parent", "left", "right" (i32[2n-1]), "aabb"
+ * (f32[8(2n-1)], min xyz 0 max xyz 0), "sizes" (u32[2n-1]), "morton" (u64[n], sorted),
+ * "sites_sorted" (f64[4(n+6)]), "status" (u8[n]), "knn" (u32[n*k]), "known_radii"
+ * (f32[n]), "vertex_nb", "edge_nb" (u32[n]), "vertices", "edges" (u32 records of 4 words,
+ * cells in sorted order, sorted-space ids). With dst == NULL only *count is set (elements). */
+apo2_status apo2_debug_array( apo2_handle * h, const char * name, void * dst, uint64_t capacity_bytes,
+                              uint64_t * count );
+
+apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats );
+
+apo2_status apo2_destroy( apo2_handle * h );
+
+/* One-call forms of the reference's free functions (apo/include/apo/gpu/algorithm.hpp:58-59):
+ * build the diagram of host sites and copy the vertices (and closed edges) out. The output
+ * arrays are allocated with malloc and released with apo2_free. */
+apo2_status apo2_compute_diagram( const void * sites, uint32_t n, apo2_dtype dtype, double ** positions,
+                                  uint32_t ** ids, uint64_t * count );
+apo2_status apo2_compute_full_diagram( const void * sites, uint32_t n, apo2_dtype dtype, double ** positions,
+                                       uint32_t ** ids, uint64_t * count, double ** closed_positions,
+                                       uint32_t ** closed_ids, uint64_t * closed_count );
+void apo2_free( void * p );
+
+/* LBVH only (apo/src/gpu/lbvh.cu:274-323): Morton codes of device float4 sites inside the
+ * scene box, stable onesweep radix sort, Karras hierarchy and refit. All pointers are device
+ * pointers of the sizes given in apo2_debug_array's list; `scratch` is a device buffer of at
+ * least apo2_lbvh_scratch_bytes(n) bytes. */
+uint64_t    apo2_lbvh_scratch_bytes( uint32_t n );
+apo2_status apo2_lbvh_build( const float * sites_xyzr, uint32_t n, const float scene_min[ 3 ],
+                             const float scene_max[ 3 ], uint32_t * indices, uint64_t * sorted_codes,
+                             int32_t * parent, int32_t * left, int32_t * right, float * aabb, uint32_t * sizes,
+                             void * scratch, void * stream );
+
+/* Stable radix sort of (u64 key, u32 value) pairs by key on the device (the LBVH's sort):
+ * keys/values are sorted in place; `scratch` must hold apo2_radix_sort_scratch_bytes(n). */
+uint64_t    apo2_radix_sort_scratch_bytes( uint32_t n );
+apo2_status apo2_radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t n, void * scratch, void * stream );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APO2_H */

@@ -1,0 +1,82 @@
+"""ctypes binding of the CPU oracle (oracle/apo_oracle.cpp) -- test infrastructure only.
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's CPU legs as the checker or the
+timed CPU baseline. The product (apo_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "build", "libapo_oracle.so")
+
+STAGE_LBVH, STAGE_KNN, STAGE_CELLS, STAGE_VALIDATION, STAGE_OUTPUT = 1, 2, 3, 4, 5
+
+_ARRAYS = {
+    "indices": np.uint32, "morton": np.uint64, "parent": np.int32, "left": np.int32,
+    "right": np.int32, "aabb": np.float32, "sizes": np.uint32, "sites_sorted": np.float64,
+    "status": np.uint8, "knn": np.uint32, "known_radii": np.float32, "vertex_nb": np.uint32,
+    "edge_nb": np.uint32, "vertices": np.uint32, "edges": np.uint32,
+    "out_vertices": np.float64, "out_vertices_id": np.uint32, "out_closed": np.float64,
+    "out_closed_id": np.uint32, "topo_quad": np.uint32, "topo_tri": np.uint32,
+    "topo_bi": np.uint32,
+}
+
+_lib = None
+
+
+def build_library() -> str:
+    """Compiles the oracle with its Makefile (g++, OpenMP); returns the library path."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build_library()
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.oracle_build.restype = ctypes.c_void_p
+        lib.oracle_build.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]
+        lib.oracle_build_f64.restype = ctypes.c_void_p
+        lib.oracle_build_f64.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]
+        lib.oracle_get.restype = ctypes.c_uint64
+        lib.oracle_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]
+        lib.oracle_flags.restype = ctypes.c_uint32
+        lib.oracle_flags.argtypes = [ctypes.c_void_p]
+        lib.oracle_free.argtypes = [ctypes.c_void_p]
+        _lib = lib
+    return _lib
+
+
+def build(sites: np.ndarray, stage: int = STAGE_OUTPUT, threads: int = 0) -> dict:
+    """Runs the oracle on float32 (n, 4) sites; returns every result array by name."""
+    lib = _load()
+    sites = np.ascontiguousarray(sites)
+    n = sites.shape[0]
+    if sites.dtype == np.float64:
+        handle = lib.oracle_build_f64(sites.ctypes.data, n, stage, threads)
+    else:
+        sites = np.ascontiguousarray(sites, dtype=np.float32)
+        handle = lib.oracle_build(sites.ctypes.data, n, stage, threads)
+    if not handle:
+        raise ValueError("oracle rejected the input")
+    try:
+        out = {}
+        for name, dtype in _ARRAYS.items():
+            ptr = ctypes.c_void_p()
+            count = lib.oracle_get(handle, name.encode(), ctypes.byref(ptr))
+            if count and ptr.value:
+                buf = (ctypes.c_char * (count * np.dtype(dtype).itemsize)).from_address(ptr.value)
+                out[name] = np.frombuffer(bytes(buf), dtype=dtype).copy()
+            else:
+                out[name] = np.zeros(0, dtype=dtype)
+        out["flags"] = int(lib.oracle_flags(handle))
+        return out
+    finally:
+        lib.oracle_free(handle)

@@ -1,0 +1,242 @@
+// Driver for the reference library built from its own sources (oracle/ref_build.sh).
+//
+// It runs the reference's public path -- `AlgorithmGPU<16>{sites}.build()` followed by
+// `toHostFull()` and `toTopology()` (apo/include/apo/gpu/algorithm.inl:1410-1821) -- on a
+// site file and writes every array the parity tests pin: the LBVH node arrays and the
+// Morton permutation (apo/src/gpu/lbvh.cu:274-323), the kNN lists of the first search
+// round (apo/include/apo/gpu/algorithm.inl:32-99), the per-cell vertex and edge stores,
+// the cell status bytes, the full diagram and the topology. With --time it also times the
+// reference's own benchmark region (constructor + build(),
+// app/benchmarks/benchmark.cu:9-22) with CUDA events.
+//
+// This is test infrastructure: it only produces golden data and the reference GPU
+// timing beside the product's numbers; nothing in the product links it.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "apo/gpu/algorithm.cuh"
+
+namespace
+{
+    template<class T>
+    void writeArray( const std::string & dir, const char * name, const T * data, std::size_t count )
+    {
+        const std::string path = dir + "/" + name;
+        FILE *            f    = std::fopen( path.c_str(), "wb" );
+        if ( !f )
+        {
+            std::fprintf( stderr, "cannot open %s\n", path.c_str() );
+            std::exit( 3 );
+        }
+        if ( count )
+            std::fwrite( data, sizeof( T ), count, f );
+        std::fclose( f );
+    }
+
+    template<class T>
+    std::vector<T> download( const T * device, std::size_t count )
+    {
+        std::vector<T> host( count );
+        if ( count )
+            cudaMemcpy( host.data(), device, count * sizeof( T ), cudaMemcpyDeviceToHost );
+        return host;
+    }
+
+    void check( const char * what )
+    {
+        const cudaError_t err = cudaDeviceSynchronize();
+        if ( err != cudaSuccess )
+        {
+            std::fprintf( stderr, "%s: %s\n", what, cudaGetErrorString( err ) );
+            std::exit( 4 );
+        }
+    }
+} // namespace
+
+int main( int argc, char ** argv )
+{
+    if ( argc < 3 )
+    {
+        std::fprintf( stderr, "usage: %s sites.f32 outdir [--time R] [--no-dump]\n", argv[ 0 ] );
+        return 1;
+    }
+    const std::string input  = argv[ 1 ];
+    const std::string outDir = argv[ 2 ];
+    int               repeat = 0;
+    bool              dump   = true;
+    for ( int a = 3; a < argc; a++ )
+    {
+        if ( !std::strcmp( argv[ a ], "--time" ) && a + 1 < argc )
+            repeat = std::atoi( argv[ ++a ] );
+        else if ( !std::strcmp( argv[ a ], "--no-dump" ) )
+            dump = false;
+    }
+
+    // Sites are stored as float32 (x, y, z, r); the reference's FP64 build reads `double`.
+    FILE * f = std::fopen( input.c_str(), "rb" );
+    if ( !f )
+    {
+        std::fprintf( stderr, "cannot open %s\n", input.c_str() );
+        return 2;
+    }
+    std::fseek( f, 0, SEEK_END );
+    const long bytes = std::ftell( f );
+    std::fseek( f, 0, SEEK_SET );
+    std::vector<float> raw( static_cast<std::size_t>( bytes ) / sizeof( float ) );
+    if ( std::fread( raw.data(), sizeof( float ), raw.size(), f ) != raw.size() )
+        return 2;
+    std::fclose( f );
+    std::vector<apo::Real> sites( raw.begin(), raw.end() );
+    const uint32_t         n = static_cast<uint32_t>( sites.size() / 4 );
+
+    std::string json = "{\"n\": " + std::to_string( n );
+
+    if ( repeat > 0 )
+    {
+        cudaEvent_t start, stop;
+        cudaEventCreate( &start );
+        cudaEventCreate( &stop );
+        std::vector<float> times;
+        double stage[ 7 ] = { 0, 0, 0, 0, 0, 0, 0 };
+        for ( int r = -3; r < repeat; r++ )
+        {
+            cudaDeviceSynchronize();
+            cudaEventRecord( start );
+            {
+                apo::gpu::AlgorithmGPU<16> algorithm { apo::ConstSpan<apo::Real> { sites.data(), sites.size() } };
+                algorithm.build();
+                if ( r >= 0 )
+                {
+                    stage[ 0 ] += algorithm.sample.initialization;
+                    stage[ 1 ] += algorithm.sample.bvhConstruction;
+                    stage[ 2 ] += algorithm.sample.knnSearch;
+                    stage[ 3 ] += algorithm.sample.knnConstruction;
+                    stage[ 4 ] += algorithm.sample.vertexValidation;
+                    stage[ 5 ] += algorithm.sample.edgeValidation;
+                    stage[ 6 ] += algorithm.sample.bisectorValidation;
+                }
+            }
+            cudaEventRecord( stop );
+            cudaEventSynchronize( stop );
+            float ms = 0.f;
+            cudaEventElapsedTime( &ms, start, stop );
+            if ( r >= 0 )
+                times.push_back( ms );
+        }
+        check( "timed builds" );
+        std::sort( times.begin(), times.end() );
+        char buffer[ 512 ];
+        std::snprintf( buffer,
+                       sizeof( buffer ),
+                       ", \"build_ms_median\": %.6f, \"build_ms_min\": %.6f, \"repeat\": %d, \"stage_ms\": {"
+                       "\"initialization\": %.6f, \"bvh\": %.6f, \"knn_search\": %.6f, \"knn_cells\": %.6f, "
+                       "\"vertex_validation\": %.6f, \"edge_validation\": %.6f, \"bisector_validation\": %.6f}",
+                       times[ times.size() / 2 ],
+                       times.front(),
+                       repeat,
+                       stage[ 0 ] / repeat,
+                       stage[ 1 ] / repeat,
+                       stage[ 2 ] / repeat,
+                       stage[ 3 ] / repeat,
+                       stage[ 4 ] / repeat,
+                       stage[ 5 ] / repeat,
+                       stage[ 6 ] / repeat );
+        json += buffer;
+    }
+
+    if ( dump )
+    {
+        apo::gpu::AlgorithmGPU<16> algorithm { apo::ConstSpan<apo::Real> { sites.data(), sites.size() } };
+        algorithm.build();
+        check( "build" );
+
+        const uint32_t nodeCount = 2 * n - 1;
+        const auto     view      = algorithm.bvh.getDeviceView();
+        {
+            const auto indices = download( view.indices, n );
+            writeArray( outDir, "indices.u32", indices.data(), indices.size() );
+            const auto parent = download( view.nodesParent, nodeCount );
+            writeArray( outDir, "parent.i32", parent.data(), parent.size() );
+            const auto left = download( view.nodesLeft, nodeCount );
+            writeArray( outDir, "left.i32", left.data(), left.size() );
+            const auto right = download( view.nodesRight, nodeCount );
+            writeArray( outDir, "right.i32", right.data(), right.size() );
+            const auto aabb = download( view.nodesAabb, 2 * std::size_t( nodeCount ) );
+            writeArray( outDir, "aabb.f32", reinterpret_cast<const float *>( aabb.data() ), aabb.size() * 4 );
+            const auto sizes = download( view.sizes, nodeCount );
+            writeArray( outDir, "sizes.u32", sizes.data(), sizes.size() );
+        }
+
+        const auto sorted = download( algorithm.dSites.get<apo::Real>(), ( n + 6 ) * 4 );
+        writeArray( outDir, "sites_sorted.f64", sorted.data(), sorted.size() );
+
+        const auto status = download( algorithm.dStatus.get<uint8_t>(), n );
+        writeArray( outDir, "status.u8", status.data(), status.size() );
+
+        const auto vertexNb = download( algorithm.dVerticesNb.get<uint32_t>(), n );
+        const auto edgeNb   = download( algorithm.dEdgesNb.get<uint32_t>(), n );
+        writeArray( outDir, "vertex_nb.u32", vertexNb.data(), vertexNb.size() );
+        writeArray( outDir, "edge_nb.u32", edgeNb.data(), edgeNb.size() );
+        {
+            const auto vertexStore = download( algorithm.dVertices.get<uint32_t>(), std::size_t( n ) * 152 * 4 );
+            const auto edgeStore   = download( algorithm.dEdges.get<uint32_t>(), std::size_t( n ) * 264 * 4 );
+            std::vector<uint32_t> vertices, edges;
+            for ( uint32_t i = 0; i < n; i++ )
+            {
+                const uint32_t vn = std::min( vertexNb[ i ], 152u );
+                const uint32_t en = std::min( edgeNb[ i ], 264u );
+                vertices.insert( vertices.end(),
+                                 vertexStore.begin() + std::size_t( i ) * 152 * 4,
+                                 vertexStore.begin() + std::size_t( i ) * 152 * 4 + vn * 4 );
+                edges.insert( edges.end(),
+                              edgeStore.begin() + std::size_t( i ) * 264 * 4,
+                              edgeStore.begin() + std::size_t( i ) * 264 * 4 + en * 4 );
+            }
+            writeArray( outDir, "vertices.u32", vertices.data(), vertices.size() );
+            writeArray( outDir, "edges.u32", edges.data(), edges.size() );
+        }
+
+        // kNN lists of the first round: relaunch the reference's own kNN kernel on the final
+        // context (it only re-marks buried cells, which are already marked).
+        {
+            apo::gpu::ContextCellOriented context {};
+            context.siteNb   = n;
+            context.sites    = algorithm.dSites.get<apo::gpu::Real4>();
+            context.status   = algorithm.dStatus.get<uint8_t>();
+            uint32_t * knns  = nullptr;
+            cudaMalloc( &knns, sizeof( uint32_t ) * n * 16 );
+            cudaMemset( knns, 0xff, sizeof( uint32_t ) * n * 16 );
+            auto [ gridDim, blockDim ] = apo::gpu::KernelConfig::From( n, apo::gpu::impl::KnnBlockSize );
+            apo::gpu::impl::getKnns<16><<<gridDim, blockDim>>>( 0, context, view, knns );
+            check( "getKnns" );
+            const auto knnHost = download( knns, std::size_t( n ) * 16 );
+            writeArray( outDir, "knn.u32", knnHost.data(), knnHost.size() );
+            cudaFree( knns );
+        }
+
+        const apo::gpu::FullDiagram full = algorithm.toHostFull( true );
+        check( "toHostFull" );
+        writeArray( outDir, "vertices_pos.f64", full.vertices.data(), full.vertices.size() );
+        writeArray( outDir, "vertices_id.u32", full.verticesId.data(), full.verticesId.size() );
+        writeArray( outDir, "closed_pos.f64", full.closedEdgesMin.data(), full.closedEdgesMin.size() );
+        writeArray( outDir, "closed_id.u32", full.closedEdgesId.data(), full.closedEdgesId.size() );
+
+        const apo::gpu::Topology topology = algorithm.toTopology();
+        writeArray( outDir, "topo_quad.u32", topology.quadrisectors.data(), topology.quadrisectors.size() );
+        writeArray( outDir, "topo_tri.u32", topology.trisectors.data(), topology.trisectors.size() );
+        writeArray( outDir, "topo_bi.u32", topology.bisectors.data(), topology.bisectors.size() );
+
+        json += ", \"vertices\": " + std::to_string( full.vertices.size() / 4 );
+        json += ", \"closed_edges\": " + std::to_string( full.closedEdgesMin.size() / 4 );
+    }
+
+    json += "}\n";
+    writeArray( outDir, "meta.json", json.data(), json.size() );
+    std::fputs( json.c_str(), stdout );
+    return 0;
+}

@@ -1,0 +1,94 @@
+"""Turns dumps of the reference library into the committed golden fixtures.
+
+The dumps come from oracle/_ref/apo_ref_driver (the reference's own CUDA sources built by
+oracle/ref_build.sh, run on a B200): `apo_ref_driver sites.f32 outdir` writes the LBVH
+arrays, the kNN lists, the per-cell stores, the full diagram and the topology of the
+reference's FP64 `AlgorithmGPU<16>` build. The input sites are generated by
+apo_b200.generators (named in CASES below), so only the outputs are stored.
+
+Small cases are stored whole (compressed .npz). For every case, each array's SHA-256 is
+recorded in digests.json, so larger cases are pinned without storing their arrays.
+
+Usage: python tests/golden/make_golden.py <dump_root>   (dump_root/<case>/*.u32 ...)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from apo_b200 import generators  # noqa: E402
+
+# case -> (generator expression, store whole arrays)
+CASES = {
+    "prec0": ("precision_cloud(0)", True),
+    "prec1": ("precision_cloud(1)", True),
+    "prec2": ("precision_cloud(2)", True),
+    "prec3": ("precision_cloud(3)", True),
+    "uni2k": ("uniform_cloud(2000, 58.48, 1.5, 0.5)", True),
+    "uniform_small": ("uniform_small()", False),
+}
+
+ARRAYS = {
+    "indices": np.uint32, "parent": np.int32, "left": np.int32, "right": np.int32,
+    "aabb": np.float32, "sizes": np.uint32, "sites_sorted": np.float64, "knn": np.uint32,
+    "status": np.uint8, "vertex_nb": np.uint32, "edge_nb": np.uint32, "vertices": np.uint32,
+    "edges": np.uint32, "vertices_id": np.uint32, "vertices_pos": np.float64,
+    "closed_id": np.uint32, "closed_pos": np.float64, "topo_quad": np.uint32,
+    "topo_tri": np.uint32, "topo_bi": np.uint32,
+}
+_EXT = {np.uint32: "u32", np.int32: "i32", np.float32: "f32", np.float64: "f64", np.uint8: "u8"}
+
+
+def sites_for(case: str) -> np.ndarray:
+    return eval("generators." + CASES[case][0])  # noqa: S307 - fixed table above
+
+
+def load_dump(root: str, case: str) -> dict:
+    out = {}
+    for name, dt in ARRAYS.items():
+        path = os.path.join(root, case, f"{name}.{_EXT[dt]}")
+        a = np.fromfile(path, dtype=dt)
+        if name == "closed_id":
+            # the reference leaves the 4th id word uninitialised; only (i, j, k) is defined
+            a = a.reshape(-1, 4)[:, :3].copy().reshape(-1)
+        out[name] = a
+    return out
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def main(root: str) -> None:
+    digests = {}
+    for case, (_, whole) in CASES.items():
+        if not os.path.isdir(os.path.join(root, case)):
+            print("skip", case)
+            continue
+        sites = sites_for(case)
+        dump = load_dump(root, case)
+        meta = json.load(open(os.path.join(root, case, "meta.json")))
+        digests[case] = {
+            "n": int(sites.shape[0]),
+            "sites_sha256": digest(sites),
+            "vertices": int(meta.get("vertices", 0)),
+            "closed_edges": int(meta.get("closed_edges", 0)),
+            "arrays": {k: digest(v) for k, v in dump.items()},
+            "sizes": {k: int(v.size) for k, v in dump.items()},
+        }
+        if whole:
+            np.savez_compressed(os.path.join(HERE, f"{case}.npz"), **dump)
+        print(case, sites.shape[0], "stored" if whole else "digests only")
+    with open(os.path.join(HERE, "digests.json"), "w") as f:
+        json.dump(digests, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1])

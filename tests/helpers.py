@@ -1,0 +1,61 @@
+"""Shared helpers of the parity tests: golden fixtures and canonical comparisons."""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+# Cases stored whole under tests/golden (reference dumps), and those pinned by digest only.
+STORED_CASES = ["prec0", "prec1", "prec2", "prec3", "uni2k"]
+DIGEST_CASES = ["uniform_small"]
+
+# Bit-exact arrays (integer / index work, and float arrays produced by exact operations).
+EXACT = ["indices", "parent", "left", "right", "aabb", "sizes", "sites_sorted", "knn", "status",
+         "vertex_nb", "edge_nb", "vertices", "edges", "topo_quad", "topo_tri", "topo_bi"]
+
+# Vertex positions of the CPU oracle against the reference: the oracle evaluates double
+# arithmetic without fused multiply-adds and single-precision square roots with IEEE sqrtf
+# (the reference uses the approximate hardware root), so positions agree to this relative
+# tolerance (the north-star bound is 1e-5 relative).
+ORACLE_POSITION_RTOL = 1e-5
+
+
+def load_golden(case: str) -> dict:
+    with np.load(os.path.join(GOLDEN, case + ".npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+def digests() -> dict:
+    with open(os.path.join(GOLDEN, "digests.json")) as f:
+        return json.load(f)
+
+
+def sites_for(case: str) -> np.ndarray:
+    from tests.golden.make_golden import sites_for as _s
+    return _s(case)
+
+
+def sha(a: np.ndarray) -> str:
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def closed_ids3(a: np.ndarray) -> np.ndarray:
+    return a.reshape(-1, 4)[:, :3].copy().reshape(-1)
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    a = a.reshape(-1, 4)
+    b = b.reshape(-1, 4)
+    if a.size == 0:
+        return 0.0
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b))))
+
+
+def canonical_rows(a: np.ndarray, width: int) -> np.ndarray:
+    """Sorts ids inside each tuple, then the tuples (for order-free topology comparison)."""
+    r = np.sort(a.reshape(-1, width), axis=1)
+    return r[np.lexsort(r.T[::-1])]
