@@ -18,7 +18,8 @@
 
 namespace apo2
 {
-    constexpr uint32_t kFull = 0xffffffffu;
+    constexpr uint32_t kFull        = 0xffffffffu;
+    constexpr uint32_t kMaxRestarts = 4096; // bound of the restart loops of the edge / bisector passes
 
     __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
     __device__ __forceinline__ uint32_t highest( uint32_t m ) { return 31u - __clz( m ); }
@@ -663,8 +664,14 @@ namespace apo2
         int            sp   = 0;
         uint32_t       node = 0;
         const float    start = -FLT_MAX;
+        uint32_t       steps = 0;
         while ( true )
         {
+            if ( ++steps > 4 * n + 64 )
+            {
+                err |= kErrWalk;
+                break;
+            }
             while ( node < n - 1 )
             {
                 Box      lb, rb;
@@ -781,10 +788,17 @@ namespace apo2
         for ( uint32_t i = gwarp; i < c.n; i += nwarp )
         {
             const uint8_t status = c.status[ i ];
-            if ( status == kFullyValidated || status == kBuried )
+            if ( status == kFullyValidated )
                 continue;
             const double4 si = c.sites[ i ];
             initial_cell( c, w, si );
+            if ( status == kBuried )
+            {
+                // a buried cell keeps the initial store (topology_update.inl:5-47)
+                store_cell( c, w, i, 0, err );
+                __syncwarp();
+                continue;
+            }
             double known = -DBL_MAX;
             for ( uint32_t q = 0; q < c.k; q++ )
             {
@@ -866,8 +880,14 @@ namespace apo2
                 float    best     = FLT_MAX;
                 uint32_t neighbor = kNone;
                 bool     walking  = need;
+                uint32_t steps = 0;
                 while ( true )
                 {
+                    if ( walking && ++steps > 4 * n + 64 )
+                    {
+                        err |= kErrWalk;
+                        walking = false;
+                    }
                     while ( walking && node < n - 1 )
                     {
                         Box      lb, rb;
@@ -986,6 +1006,7 @@ namespace apo2
             __syncwarp();
             bool           changedCell = false;
             const uint32_t steps       = w.en / 32 + 1;
+            uint32_t       restarts    = 0;
             for ( uint32_t es = 0; es < steps; es++ )
             {
                 const uint32_t eid  = es * 32 + lane;
@@ -1046,8 +1067,14 @@ namespace apo2
                 uint32_t node    = 0;
                 uint32_t found   = kNone;
                 bool     walking = need;
+                uint32_t steps = 0;
                 while ( true )
                 {
+                    if ( walking && ++steps > 4 * n + 64 )
+                    {
+                        err |= kErrWalk;
+                        walking = false;
+                    }
                     while ( walking && node < n - 1 )
                     {
                         Box      lb, rb;
@@ -1155,7 +1182,15 @@ namespace apo2
                     const bool changed = update_cell( c, w, i, si, tj, c.sites[ tj ], err );
                     changedCell        = changedCell || changed;
                     if ( changed )
+                    {
                         es = 0; // the reference restarts here; the loop's increment follows
+                        if ( ++restarts > kMaxRestarts )
+                        {
+                            err |= kErrWalk;
+                            es = steps;
+                            break;
+                        }
+                    }
                 }
             }
             const uint32_t base = c.vertex_nb[ i ];
@@ -1260,6 +1295,7 @@ namespace apo2
             const float  fri = float( si.w );
             bool         changedCell = false;
             const uint32_t steps     = bisectorNb / 32 + 1;
+            uint32_t       restarts  = 0;
             for ( uint32_t bs = 0; bs < steps; bs++ )
             {
                 const uint32_t bid      = bs * 32 + lane;
@@ -1300,8 +1336,14 @@ namespace apo2
                 uint32_t node    = 0;
                 uint32_t found   = kNone;
                 bool     walking = need;
+                uint32_t steps = 0;
                 while ( true )
                 {
+                    if ( walking && ++steps > 4 * n + 64 )
+                    {
+                        err |= kErrWalk;
+                        walking = false;
+                    }
                     while ( walking && node < n - 1 )
                     {
                         Box      lb, rb;
@@ -1399,7 +1441,15 @@ namespace apo2
                     const bool changed = update_cell( c, w, i, si, tj, c.sites[ tj ], err );
                     changedCell        = changedCell || changed;
                     if ( changed )
+                    {
                         bs = 0;
+                        if ( ++restarts > kMaxRestarts )
+                        {
+                            err |= kErrWalk;
+                            bs = steps;
+                            break;
+                        }
+                    }
                 }
             }
             const uint32_t base = c.vertex_nb[ i ];

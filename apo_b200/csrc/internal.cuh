@@ -36,6 +36,7 @@ namespace apo2
         kErrBisector   = 8,
         kErrStack      = 16,
         kErrSortSpin   = 32,
+        kErrWalk       = 64,  // a traversal or a validation restart loop hit its bound
     };
 
     // Scene box and radius range, written on the device by the bounds kernel.

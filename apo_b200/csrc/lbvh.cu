@@ -336,8 +336,9 @@ namespace apo2
             return;
         if ( sizes )
             sizes[ leaf ] = 1;
-        int node = parent[ leaf ];
-        while ( node >= 0 && atomicAdd( &arrivals[ node ], 1u ) > 0 )
+        int      node  = parent[ leaf ];
+        uint32_t climb = 0;
+        while ( node >= 0 && atomicAdd( &arrivals[ node ], 1u ) > 0 && ++climb <= 2 * n )
         {
             __threadfence();
             const int    l  = left[ node ], r = right[ node ];

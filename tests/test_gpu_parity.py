@@ -1,0 +1,187 @@
+"""Parity of the CUDA build (through the C ABI) with the reference's outputs and the oracle.
+
+Bar: every integer / index array (LBVH, kNN lists, cell status, per-cell vertex and edge
+stores in store order, topology) bit-identical; vertex and closed-edge positions within
+POSITION_RTOL of the reference (relative to max(1, |x|)).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+# The CUDA kernels evaluate the reference's arithmetic in the reference's order with the
+# same compiler and floating-point mode, so positions are expected to agree to the last
+# bit; this bound is what the test enforces.
+POSITION_RTOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def apo():
+    import apo_b200
+    apo_b200.load_library()
+    return apo_b200
+
+
+def _check_against_golden(apo, sites, golden, label):
+    algo = apo.AlgorithmGPU(sites)
+    algo.build()
+    for name in H.EXACT:
+        if name.startswith("topo_"):
+            continue
+        mine = algo.debug_array(name)
+        assert np.array_equal(mine, golden[name]), f"{label}: {name} differs from the reference"
+    full = algo.toHostFull(True)
+    assert np.array_equal(full.verticesId, golden["vertices_id"])
+    assert np.array_equal(H.closed_ids3(full.closedEdgesId), golden["closed_id"])
+    assert H.rel_err(full.vertices, golden["vertices_pos"]) <= POSITION_RTOL
+    assert H.rel_err(full.closedEdgesMin, golden["closed_pos"]) <= POSITION_RTOL
+    topo = algo.toTopology()
+    assert np.array_equal(topo.quadrisectors, golden["topo_quad"])
+    assert np.array_equal(topo.trisectors, golden["topo_tri"])
+    assert np.array_equal(topo.bisectors, golden["topo_bi"])
+    assert algo.stats()["error_flags"] == 0
+    algo.close()
+
+
+@pytest.mark.parametrize("case", H.STORED_CASES)
+def test_gpu_matches_reference_dump(apo, case):
+    _check_against_golden(apo, H.sites_for(case), H.load_golden(case), case)
+
+
+@pytest.mark.parametrize("case", H.STORED_CASES[:2])
+def test_gpu_float64_input_matches(apo, case):
+    """The FP64 entry (the reference's `Real` = double) gives the same diagram."""
+    _check_against_golden(apo, H.sites_for(case).astype(np.float64), H.load_golden(case), case + "/f64")
+
+
+@pytest.mark.parametrize("case", H.DIGEST_CASES)
+def test_gpu_matches_reference_digests(apo, case):
+    d = H.digests()[case]
+    algo = apo.AlgorithmGPU(H.sites_for(case))
+    algo.build()
+    for name in H.EXACT:
+        if name.startswith("topo_"):
+            continue
+        assert H.sha(algo.debug_array(name)) == d["arrays"][name], f"{case}: {name}"
+    full = algo.toHostFull(True)
+    assert H.sha(full.verticesId) == d["arrays"]["vertices_id"]
+    assert H.sha(H.closed_ids3(full.closedEdgesId)) == d["arrays"]["closed_id"]
+    topo = algo.toTopology()
+    assert H.sha(topo.quadrisectors) == d["arrays"]["topo_quad"]
+    assert H.sha(topo.trisectors) == d["arrays"]["topo_tri"]
+    assert H.sha(topo.bisectors) == d["arrays"]["topo_bi"]
+
+
+@pytest.mark.parametrize("kind,seed", [("uniform", 11), ("lognormal", 12)])
+def test_gpu_matches_oracle_seeded(apo, oracle_lib, kind, seed):
+    from apo_b200 import generators as g
+    n = 20000
+    if kind == "uniform":
+        sites = g.uniform_random(n, 127.0, 0.5, 2.0, seed)
+    else:
+        sites = g.lognormal_cloud(n, 400.0 * (n / 5e6) ** (1 / 3), seed)
+    ref = oracle_lib.build(sites)
+    algo = apo.AlgorithmGPU(sites)
+    algo.build()
+    for name in ["indices", "parent", "left", "right", "aabb", "sizes", "sites_sorted", "status", "vertex_nb",
+                 "edge_nb", "vertices", "edges"]:
+        assert np.array_equal(algo.debug_array(name), ref[name]), name
+    full = algo.toHostFull(True)
+    assert np.array_equal(full.verticesId, ref["out_vertices_id"])
+    assert H.rel_err(full.vertices, ref["out_vertices"]) <= H.ORACLE_POSITION_RTOL
+    topo = algo.toTopology()
+    assert np.array_equal(topo.quadrisectors, ref["topo_quad"])
+
+
+def test_compute_diagram_free_functions(apo):
+    golden = H.load_golden("prec1")
+    sites = H.sites_for("prec1")
+    v = apo.computeApolloniusDiagram(sites)
+    assert np.array_equal(v.verticesId, golden["vertices_id"])
+    f = apo.computeFullApolloniusDiagram(sites)
+    assert np.array_equal(f.verticesId, golden["vertices_id"])
+    assert np.array_equal(H.closed_ids3(f.closedEdgesId), golden["closed_id"])
+
+
+def test_repeated_builds_are_identical(apo):
+    sites = H.sites_for("uni2k")
+    algo = apo.AlgorithmGPU(sites)
+    algo.build()
+    first = algo.debug_array("edges").copy()
+    v1 = algo.toHost().vertices.copy()
+    for _ in range(3):
+        algo.build()
+        assert np.array_equal(algo.debug_array("edges"), first)
+        assert np.array_equal(algo.toHost().vertices, v1)
+
+
+def test_lbvh_entry_point_large(apo, oracle_lib):
+    """LBVH of 1M sites through apo2_lbvh_build, against the oracle's LBVH stage."""
+    import torch
+    from apo_b200 import generators as g
+    n = 1_000_000
+    sites = g.uniform_random(n, 464.0, 0.5, 2.0, 5)
+    ref = oracle_lib.build(sites, stage=1)
+    lo = (sites[:, :3] - sites[:, 3:]).astype(np.float64).min(axis=0).astype(np.float32)
+    hi = (sites[:, :3] + sites[:, 3:]).astype(np.float64).max(axis=0).astype(np.float32)
+    dev = torch.device("cuda:0")
+    d_sites = torch.from_numpy(sites).to(dev)
+    nodes = 2 * n - 1
+    idx = torch.empty(n, dtype=torch.int32, device=dev)
+    codes = torch.empty(n, dtype=torch.int64, device=dev)
+    parent = torch.empty(nodes, dtype=torch.int32, device=dev)
+    left = torch.empty(nodes, dtype=torch.int32, device=dev)
+    right = torch.empty(nodes, dtype=torch.int32, device=dev)
+    aabb = torch.empty(nodes * 8, dtype=torch.float32, device=dev)
+    sizes = torch.empty(nodes, dtype=torch.int32, device=dev)
+    lib = apo.load_library()
+    scratch = torch.empty(int(lib.apo2_lbvh_scratch_bytes(n)), dtype=torch.uint8, device=dev)
+    lo_c = (ctypes.c_float * 3)(*lo.tolist())
+    hi_c = (ctypes.c_float * 3)(*hi.tolist())
+    st = lib.apo2_lbvh_build(d_sites.data_ptr(), n, lo_c, hi_c, idx.data_ptr(), codes.data_ptr(), parent.data_ptr(),
+                             left.data_ptr(), right.data_ptr(), aabb.data_ptr(), sizes.data_ptr(), scratch.data_ptr(), None)
+    assert st == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(idx.cpu().numpy().view(np.uint32), ref["indices"])
+    assert np.array_equal(parent.cpu().numpy(), ref["parent"])
+    assert np.array_equal(left.cpu().numpy(), ref["left"])
+    assert np.array_equal(right.cpu().numpy(), ref["right"])
+    assert np.array_equal(sizes.cpu().numpy().view(np.uint32), ref["sizes"])
+    # the oracle restates the FP64 build (boxes from double c -/+ r); the float entry point
+    # subtracts in float, so boxes are compared on the hierarchy only above
+    mine_box = aabb.cpu().numpy().reshape(-1, 8)
+    assert np.all(mine_box[:, 0:3] <= mine_box[:, 4:7])
+
+
+def test_radix_sort_is_stable(apo):
+    import torch
+    rng = np.random.default_rng(3)
+    n = 3_000_001
+    keys = (rng.integers(0, 1 << 20, size=n, dtype=np.int64) << np.int64(30)) | rng.integers(0, 4, size=n)
+    vals = np.arange(n, dtype=np.int32)
+    dev = torch.device("cuda:0")
+    k = torch.from_numpy(keys).to(dev)
+    v = torch.from_numpy(vals).to(dev)
+    lib = apo.load_library()
+    scratch = torch.empty(int(lib.apo2_radix_sort_scratch_bytes(n)), dtype=torch.uint8, device=dev)
+    assert lib.apo2_radix_sort_pairs(k.data_ptr(), v.data_ptr(), n, scratch.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    order = np.argsort(keys.view(np.uint64), kind="stable")
+    assert np.array_equal(k.cpu().numpy(), keys[order])
+    assert np.array_equal(v.cpu().numpy(), vals[order])
+
+
+def test_invalid_arguments(apo):
+    lib = apo.load_library()
+    h = ctypes.c_void_p()
+    one = np.zeros(4, dtype=np.float32)
+    assert lib.apo2_create(one.ctypes.data, 1, 0, 0, None, ctypes.byref(h)) == apo.APO2_ERR_INVALID_ARG
+    opt = apo.Options()
+    opt.struct_size = ctypes.sizeof(apo.Options)
+    opt.k = 64
+    two = np.zeros(8, dtype=np.float32)
+    assert lib.apo2_create(two.ctypes.data, 2, 0, 0, ctypes.byref(opt), ctypes.byref(h)) == apo.APO2_ERR_INVALID_ARG
