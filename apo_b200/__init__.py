@@ -44,12 +44,13 @@ class Apo2Error(RuntimeError):
 
 class Options(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("k", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32),
-                ("device", ctypes.c_uint32), ("stage_timing", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 11)]
+                ("device", ctypes.c_uint32), ("stage_timing", ctypes.c_uint32), ("edge_search", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 10)]
 
 
 class Stats(ctypes.Structure):
     _fields_ = [("n", ctypes.c_uint32), ("buried", ctypes.c_uint32), ("certified_after_knn", ctypes.c_uint32),
-                ("validation_rounds", ctypes.c_uint32), ("error_flags", ctypes.c_uint32), ("reserved0", ctypes.c_uint32),
+                ("validation_rounds", ctypes.c_uint32), ("error_flags", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
                 ("vertex_records", ctypes.c_uint64), ("edge_records", ctypes.c_uint64),
                 ("output_vertices", ctypes.c_uint64), ("output_closed_edges", ctypes.c_uint64),
                 ("ms_bounds", ctypes.c_double), ("ms_sort", ctypes.c_double), ("ms_tree", ctypes.c_double),
@@ -80,6 +81,7 @@ SIGNATURES = {
     "apo2_get_cell": (_I, [_P, _U32, _P, _U32, _P, _P, _U32, _P]),
     "apo2_debug_array": (_I, [_P, ctypes.c_char_p, _P, _U64, _P]),
     "apo2_get_stats": (_I, [_P, _P]),
+    "apo2_kernel_profile": (_I, [_P, _P, _U64, _P]),
     "apo2_destroy": (_I, [_P]),
     "apo2_compute_diagram": (_I, [_P, _U32, _I, _P, _P, _P]),
     "apo2_compute_full_diagram": (_I, [_P, _U32, _I, _P, _P, _P, _P, _P, _P]),
@@ -88,6 +90,7 @@ SIGNATURES = {
     "apo2_lbvh_build": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "apo2_radix_sort_scratch_bytes": (_U64, [_U32]),
     "apo2_radix_sort_pairs": (_I, [_P, _P, _U32, _P, _P]),
+    "apo2_generate_chains": (_I, [_U32, _U32, ctypes.c_double, _U64, _P]),
 }
 
 
@@ -153,7 +156,8 @@ class Topology:
 class AlgorithmGPU:
     """Counterpart of `apo::gpu::AlgorithmGPU<K>` (algorithm.cuh:12-46)."""
 
-    def __init__(self, sites, k: int = 16, max_iterations: int = 10, device: int = 0, stage_timing: bool = False):
+    def __init__(self, sites, k: int = 16, max_iterations: int = 10, device: int = 0, stage_timing: bool = False,
+                 edge_search: int = 0):
         lib = load_library()
         self._sites, dtype = _as_sites(sites)
         self.n = int(self._sites.shape[0])
@@ -163,6 +167,7 @@ class AlgorithmGPU:
         opt.max_iterations = max_iterations
         opt.device = device
         opt.stage_timing = 1 if stage_timing else 0
+        opt.edge_search = edge_search
         handle = ctypes.c_void_p()
         _check(lib.apo2_create(self._sites.ctypes.data, self.n, dtype, APO2_HOST, ctypes.byref(opt), ctypes.byref(handle)))
         self._h = handle
@@ -243,6 +248,15 @@ class AlgorithmGPU:
         out = np.zeros(count.value, dtype=dt)
         _check(self._lib.apo2_debug_array(self._h, name.encode(), out.ctypes.data, out.nbytes, ctypes.byref(count)))
         return out
+
+    def kernel_profile(self) -> dict:
+        """Kernels of the last build: launch count and, with stage_timing, per-kernel times."""
+        import json
+        length = ctypes.c_uint64()
+        _check(self._lib.apo2_kernel_profile(self._h, None, 0, ctypes.byref(length)))
+        buf = ctypes.create_string_buffer(length.value + 1)
+        _check(self._lib.apo2_kernel_profile(self._h, buf, length.value + 1, ctypes.byref(length)))
+        return json.loads(buf.value.decode())
 
     def stats(self) -> dict:
         s = Stats()

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libapo2.so")
-SOURCES = ["sort.cu", "lbvh.cu", "cells.cu", "api.cu"]
+SOURCES = ["sort.cu", "lbvh.cu", "cells.cu", "speculate.cu", "api.cu", "generators.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--use_fast_math", "-Xcompiler", "-fPIC,-O2",
          "-I", os.path.join(ROOT, "include")]
@@ -46,7 +46,11 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     procs = []
     for src in SOURCES:
         obj = os.path.join(obj_dir, src + ".o")
-        cmd = [nvcc, *ARCH, *FLAGS, *(extra or []), "-c", os.path.join(CSRC, src), "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-I", os.path.join(ROOT, "include"), "-c",
+                   os.path.join(CSRC, src), "-o", obj]
+        else:
+            cmd = [nvcc, *ARCH, *FLAGS, *(extra or []), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))

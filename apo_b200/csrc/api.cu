@@ -1,5 +1,6 @@
 // C ABI of the builder (include/apo2.h): handle lifetime, device memory, the build
 // sequence on one stream, output extraction and the host-side topology.
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -79,6 +80,7 @@ struct apo2_handle
     uint32_t *     task_counts = nullptr; // one per validation round
     uint32_t *     error       = nullptr;
 
+    SpecBuffers   spec;
     OutputBuffers out;
     void *        out_alloc = nullptr;
     bool          built     = false;
@@ -87,6 +89,17 @@ struct apo2_handle
     cudaEvent_t events[ kStages + 1 ] = {};
     bool        timing                = false;
     apo2_stats  stats {};
+
+    // launch observer state: kernel count of the last build, and (timing on) per-launch events
+    struct KernelRecord
+    {
+        const char * name;
+        int          begin, end;
+    };
+    uint32_t                  launches = 0;
+    std::vector<cudaEvent_t>  event_pool;
+    size_t                    events_used = 0;
+    std::vector<KernelRecord> records;
 };
 
 namespace
@@ -126,6 +139,50 @@ namespace
         return APO2_OK;
     }
 
+    int take_event( apo2_handle * h )
+    {
+        if ( h->events_used == h->event_pool.size() )
+        {
+            cudaEvent_t e;
+            cudaEventCreate( &e );
+            h->event_pool.push_back( e );
+        }
+        return int( h->events_used++ );
+    }
+
+    void on_launch( const char * name, cudaStream_t s, bool after, void * ctx )
+    {
+        apo2_handle * h = static_cast<apo2_handle *>( ctx );
+        if ( !after )
+        {
+            h->launches++;
+            if ( h->timing )
+            {
+                const int e = take_event( h );
+                cudaEventRecord( h->event_pool[ e ], s );
+                h->records.push_back( { name, e, -1 } );
+            }
+        }
+        else if ( h->timing )
+        {
+            const int e = take_event( h );
+            cudaEventRecord( h->event_pool[ e ], s );
+            h->records.back().end = e;
+        }
+    }
+
+    struct ObserveScope
+    {
+        LaunchObserver saved;
+        explicit ObserveScope( apo2_handle * h )
+        {
+            saved                    = launch_observer();
+            launch_observer().hook   = on_launch;
+            launch_observer().ctx    = h;
+        }
+        ~ObserveScope() { launch_observer() = saved; }
+    };
+
     void record( apo2_handle * h, int stage, cudaStream_t s )
     {
         if ( h->timing )
@@ -135,6 +192,10 @@ namespace
     apo2_status enqueue_build( apo2_handle * h, cudaStream_t s )
     {
         const uint32_t n = h->n;
+        ObserveScope   observe( h );
+        h->launches    = 0;
+        h->events_used = 0;
+        h->records.clear();
         record( h, 0, s );
         cudaMemsetAsync( h->error, 0, sizeof( uint32_t ), s );
         launch_bounds( h->input, h->input_f64, n, h->input_d4, h->partials, h->partial_count, h->bounds_counter, h->scene,
@@ -151,7 +212,10 @@ namespace
         {
             launch_tasks( h->cells, h->tasks, h->task_counts + r, s );
             launch_vertex_validation( h->cells, h->tasks, h->task_counts + r, s );
-            launch_edge_validation( h->cells, h->tasks, h->task_counts + r, s );
+            if ( h->options.edge_search == 1 )
+                launch_edge_validation( h->cells, h->tasks, h->task_counts + r, s );
+            else
+                launch_edge_validation_speculative( h->cells, h->tasks, h->task_counts + r, h->spec, s );
         }
         record( h, 5, s );
         launch_bisector_validation( h->cells, s );
@@ -166,6 +230,7 @@ namespace
 
     apo2_status enqueue_extract( apo2_handle * h, cudaStream_t s )
     {
+        ObserveScope observe( h );
         launch_output( h->cells, h->out, s );
         record( h, 7, s );
         const cudaError_t err = cudaGetLastError();
@@ -253,6 +318,8 @@ apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_
         return fail( APO2_ERR_INVALID_ARG, "k is at most 16" );
     if ( opt.max_iterations == 0 )
         opt.max_iterations = 10;
+    if ( opt.edge_search > 1 )
+        return fail( APO2_ERR_INVALID_ARG, "edge_search is 0 or 1" );
     opt.max_iterations = std::min( opt.max_iterations, 64u );
 
     APO2_CUDA( cudaSetDevice( int( opt.device ) ), "cudaSetDevice" );
@@ -282,6 +349,7 @@ apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_
              + align256( sizeof( uint4 ) * kMaxVertices * size_t( n ) ) + align256( sizeof( uint4 ) * kMaxEdges * size_t( n ) );
     total += align256( 4 * size_t( n ) ) + align256( 4 * 64 ) + align256( 4 );
     total += align256( 4 * size_t( n ) ) * 2 + align256( 4 * scanWords * 2 ) + align256( 16 );
+    total += align256( spec_bytes( n ) );
     h->arena.size = total;
     cudaError_t err = cudaMalloc( reinterpret_cast<void **>( &h->arena.base ), total );
     if ( err != cudaSuccess )
@@ -326,10 +394,12 @@ apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_
     h->task_counts    = a.take<uint32_t>( 64 );
     h->error          = a.take<uint32_t>( 1 );
     c.error           = h->error;
+    c.scene           = h->scene;
     h->out.vcount     = a.take<uint32_t>( n );
     h->out.ccount     = a.take<uint32_t>( n );
     h->out.tile_sums  = a.take<uint32_t>( scanWords * 2 );
     h->out.totals     = a.take<uint64_t>( 2 );
+    spec_carve( h->spec, a.take<char>( spec_bytes( n ) ), n );
     sort_scratch_carve( h->sort, sortBase, n, h->error );
     if ( a.used > a.size )
     {
@@ -670,7 +740,8 @@ apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
     s.validation_rounds   = 0;
     for ( uint32_t r = 0; r < h->options.max_iterations; r++ )
         s.validation_rounds += counts[ r ] != 0;
-    s.error_flags = err;
+    s.error_flags     = err;
+    s.kernel_launches = h->launches;
     if ( h->timing )
     {
         float ms[ kStages ] = {};
@@ -688,6 +759,44 @@ apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
     return APO2_OK;
 }
 
+apo2_status apo2_kernel_profile( apo2_handle * h, char * json, uint64_t capacity, uint64_t * length )
+{
+    if ( !h )
+        return fail( APO2_ERR_INVALID_ARG, "null handle" );
+    APO2_CUDA( cudaDeviceSynchronize(), "kernel profile" );
+    std::map<std::string, std::pair<uint32_t, double>> per;
+    for ( const auto & r : h->records )
+    {
+        float ms = 0.f;
+        if ( r.end >= 0 )
+            cudaEventElapsedTime( &ms, h->event_pool[ r.begin ], h->event_pool[ r.end ] );
+        auto & x = per[ r.name ];
+        x.first++;
+        x.second += ms;
+    }
+    std::string out = "{\"launches\": " + std::to_string( h->launches ) + ", \"timed\": " + ( h->timing ? "true" : "false" )
+                      + ", \"kernels\": {";
+    bool first = true;
+    for ( const auto & kv : per )
+    {
+        char buf[ 160 ];
+        std::snprintf( buf, sizeof( buf ), "%s\"%s\": [%u, %.6f]", first ? "" : ", ", kv.first.c_str(), kv.second.first,
+                       kv.second.second );
+        out += buf;
+        first = false;
+    }
+    out += "}}";
+    if ( length )
+        *length = out.size();
+    if ( json )
+    {
+        if ( capacity <= out.size() )
+            return fail( APO2_ERR_INVALID_ARG, "profile buffer too small" );
+        std::memcpy( json, out.c_str(), out.size() + 1 );
+    }
+    return APO2_OK;
+}
+
 apo2_status apo2_destroy( apo2_handle * h )
 {
     if ( !h )
@@ -702,6 +811,8 @@ apo2_status apo2_destroy( apo2_handle * h )
         for ( auto & e : h->events )
             if ( e )
                 cudaEventDestroy( e );
+    for ( auto e : h->event_pool )
+        cudaEventDestroy( e );
     delete h;
     return APO2_OK;
 }

@@ -67,14 +67,6 @@ namespace apo2
     __device__ __forceinline__ uint32_t vtype( uint4 r ) { return r.w & 0xffu; }
     __device__ __forceinline__ uint32_t estatus( uint4 r ) { return r.w & 0xffu; }
 
-    // Position of a stored vertex: root `type` of quadrisector(si, sj, sk, sl) with the
-    // sorted ids (topology_update.inl:104-111).
-    __device__ __forceinline__ double4 solve_vertex( const CellContext & c, double4 si, uint4 r )
-    {
-        double4 x[ 2 ] = { make_double4( 0, 0, 0, 0 ), make_double4( 0, 0, 0, 0 ) };
-        quadrisector( si, site( c, r.x ), site( c, r.y ), site( c, r.z ), x[ 0 ], x[ 1 ] );
-        return vtype( r ) ? x[ 1 ] : x[ 0 ];
-    }
 
     // Default validation predicate of the cell update (topology_update.inl:578-592): no site
     // of the cell's edges other than skip1 / skip2 intersects `sphere`. Warp-collective;
@@ -880,10 +872,10 @@ namespace apo2
                 float    best     = FLT_MAX;
                 uint32_t neighbor = kNone;
                 bool     walking  = need;
-                uint32_t steps = 0;
+                uint32_t walk_steps = 0;
                 while ( true )
                 {
-                    if ( walking && ++steps > 4 * n + 64 )
+                    if ( walking && ++walk_steps > 4 * n + 64 )
                     {
                         err |= kErrWalk;
                         walking = false;
@@ -978,8 +970,15 @@ namespace apo2
     // -----------------------------------------------------------------------------------
     // Edge validation (algorithm.inl:478-857)
     // -----------------------------------------------------------------------------------
+    // `proof` (optional): what the edge-parallel search proved for these cells. It searched
+    // every edge against the neighbour set U0 of the stored cell. A site contributes to an
+    // edge only if it is not a neighbour and one of its roots is empty of every neighbour, so
+    // while the cell's neighbours still include all of U0 (updates only added some), an edge
+    // with no contributor then has none now: its search would find nothing and is skipped.
+    // Once a neighbour of U0 has left the cell, every edge is searched again.
     __global__ void __launch_bounds__( kCellBlock ) k_edge_validation( CellContext c, const uint32_t * __restrict__ tasks,
-                                                                      const uint32_t * __restrict__ task_count )
+                                                                      const uint32_t * __restrict__ task_count,
+                                                                      SearchProof proof )
     {
         extern __shared__ __align__( 16 ) unsigned char smem[];
         const uint32_t warp  = threadIdx.x >> 5;
@@ -1007,6 +1006,10 @@ namespace apo2
             bool           changedCell = false;
             const uint32_t steps       = w.en / 32 + 1;
             uint32_t       restarts    = 0;
+            bool             monotone = proof.maybe_bits != nullptr; // neighbours still include U0
+            const uint32_t   slot     = monotone ? proof.slots[ t ] : 0u;
+            const uint32_t * maybe    = monotone ? proof.maybe_bits + size_t( slot ) * kMaybeWords : nullptr;
+            const uint32_t   stored_en = w.en;
             for ( uint32_t es = 0; es < steps; es++ )
             {
                 const uint32_t eid  = es * 32 + lane;
@@ -1019,8 +1022,10 @@ namespace apo2
                     l             = r.y;
                     need          = estatus( r ) == 2;
                 }
-                uint32_t type = 0;
+                uint32_t type = 0, cnt = 0;
                 double4  ev0 = make_double4( 0, 0, 0, 0 ), ev1 = make_double4( 0, 0, 0, 0 );
+                if ( eid < w.en )
+                    cnt = w.e[ eid ].z;
                 double4  sk = make_double4( 0, 0, 0, 0 ), sl = make_double4( 0, 0, 0, 0 );
                 if ( need )
                 {
@@ -1060,17 +1065,69 @@ namespace apo2
                     w.e[ eid ].w = ( w.e[ eid ].w & 0xffffff00u ) | 1u;
                     need         = false;
                 }
+                // reach of the search (see reach_radius): the stored vertices and the ones
+                // added by this pass that lie on the edge, and its possible apexes
+                float4 reach = make_float4( fsi.x, fsi.y, fsi.z, 0.f );
+                if ( need )
+                {
+                    double         wmax = 0.0;
+                    const uint32_t svn  = c.vertex_nb[ i ];
+                    for ( uint32_t v = 0; v < svn; v++ )
+                    {
+                        const uint4 r = c.vertices[ size_t( i ) * kMaxVertices + v ];
+                        if ( vertex_on_edge( r, k, l ) )
+                            wmax = fmax( wmax, solve_vertex( c, si, r ).w );
+                    }
+                    for ( uint32_t v = 0; v < w.vn; v++ )
+                        if ( vertex_on_edge( w.v[ v ], k, l ) )
+                            wmax = fmax( wmax, w.pos[ v ].w );
+                    if ( ellipse || cnt == kNone )
+                    {
+                        const double4 apex[ 2 ] = { ev0, ev1 };
+                        for ( uint32_t a = 0; a < 2; a++ )
+                        {
+                            bool out = false;
+                            for ( uint32_t e2 = 0; e2 < w.en && !out; e2++ )
+                            {
+                                const uint4 r2 = w.e[ e2 ];
+                                if ( r2.x != k && r2.x != l )
+                                    out = clearly_outside( c.sites[ r2.x ], apex[ a ] );
+                                if ( !out && r2.y != k && r2.y != l )
+                                    out = clearly_outside( c.sites[ r2.y ], apex[ a ] );
+                            }
+                            if ( !out )
+                                wmax = fmax( wmax, apex[ a ].w );
+                        }
+                    }
+                    reach.w = reach_radius( wmax, si.w, c.scene->rmax );
+                }
+
+                // proven free of contributors on this very cell state
+                bool skip = false;
+                if ( monotone && need )
+                {
+                    // the edge's index in the stored cell, where the proof's bits refer
+                    for ( uint32_t e0 = 0; e0 < stored_en; e0++ )
+                    {
+                        const uint4 r0 = c.edges[ size_t( i ) * kMaxEdges + e0 ];
+                        if ( r0.x == k && r0.y == l )
+                        {
+                            skip = !( ( maybe[ e0 >> 5 ] >> ( e0 & 31 ) ) & 1u );
+                            break;
+                        }
+                    }
+                }
 
                 // first site inside the bounding volume that gives the edge two valid vertices
                 uint32_t stack[ kStack ];
                 int      sp      = 0;
                 uint32_t node    = 0;
                 uint32_t found   = kNone;
-                bool     walking = need;
-                uint32_t steps = 0;
+                bool     walking = need && !skip;
+                uint32_t walk_steps = 0;
                 while ( true )
                 {
-                    if ( walking && ++steps > 4 * n + 64 )
+                    if ( walking && ++walk_steps > 4 * n + 64 )
                     {
                         err |= kErrWalk;
                         walking = false;
@@ -1092,6 +1149,8 @@ namespace apo2
                         bool exploreClose = minClose < 0.f;
                         if ( hyperbola && exploreClose )
                             exploreClose = fdot( n1, closePoint - pp1 ) < 0.f && fdot( n2, closePoint - pp2 ) < 0.f;
+                        exploreFar   = exploreFar && ( leftClosest ? rb : lb ).distance( reach ) < 0.f;
+                        exploreClose = exploreClose && ( leftClosest ? lb : rb ).distance( reach ) < 0.f;
                         if ( !exploreFar && !exploreClose )
                             break;
                         node = exploreClose ? closeChild : farChild;
@@ -1111,7 +1170,7 @@ namespace apo2
                     {
                         sj              = c.sites[ j ];
                         const float4 fj = to_float( sj );
-                        can             = intersects( fj, bsph );
+                        can             = intersects( fj, bsph ) && flength( f3( fj ) - f3( reach ) ) <= reach.w;
                         if ( hyperbola )
                             can = can && double( fdot( n1, f3( fj ) - pp1 ) ) < -sj.w
                                   && double( fdot( n2, f3( fj ) - pp2 ) ) < -sj.w;
@@ -1180,6 +1239,13 @@ namespace apo2
                     if ( is_known( w, tj ) )
                         continue;
                     const bool changed = update_cell( c, w, i, si, tj, c.sites[ tj ], err );
+                    if ( monotone )
+                    {
+                        const uint32_t   cnt0 = proof.nbr_count[ slot ];
+                        const uint32_t * u0   = proof.nbr + size_t( slot ) * kNbrCap;
+                        for ( uint32_t q = 0; q < cnt0 && monotone; q++ )
+                            monotone = is_known( w, u0[ q ] );
+                    }
                     changedCell        = changedCell || changed;
                     if ( changed )
                     {
@@ -1336,10 +1402,10 @@ namespace apo2
                 uint32_t node    = 0;
                 uint32_t found   = kNone;
                 bool     walking = need;
-                uint32_t steps = 0;
+                uint32_t walk_steps = 0;
                 while ( true )
                 {
-                    if ( walking && ++steps > 4 * n + 64 )
+                    if ( walking && ++walk_steps > 4 * n + 64 )
                     {
                         err |= kErrWalk;
                         walking = false;
@@ -1675,12 +1741,12 @@ namespace apo2
 
     size_t output_scan_scratch_words( uint32_t n ) { return ( n + kScanTile - 1 ) / kScanTile + 1; }
 
-    static void scan_exclusive( uint32_t * data, uint32_t n, uint32_t * sums, uint64_t * total, cudaStream_t s )
+    void scan_exclusive( uint32_t * data, uint32_t n, uint32_t * sums, uint64_t * total, cudaStream_t s )
     {
         const uint32_t tiles = std::max( 1u, ( n + kScanTile - 1 ) / kScanTile );
-        k_tile_sums<<<tiles, kScanBlock, 0, s>>>( data, n, sums );
-        k_scan_tile_sums<<<1, kScanBlock, 0, s>>>( sums, tiles, total );
-        k_scan_tiles<<<tiles, kScanBlock, 0, s>>>( data, n, sums );
+        APO2_LAUNCH( "k_tile_sums", s, k_tile_sums<<<tiles, kScanBlock, 0, s>>>( data, n, sums ) );
+        APO2_LAUNCH( "k_scan_tile_sums", s, k_scan_tile_sums<<<1, kScanBlock, 0, s>>>( sums, tiles, total ) );
+        APO2_LAUNCH( "k_scan_tiles", s, k_scan_tiles<<<tiles, kScanBlock, 0, s>>>( data, n, sums ) );
     }
 
     // -----------------------------------------------------------------------------------
@@ -1713,42 +1779,43 @@ namespace apo2
 
     void launch_knn( const CellContext & c, cudaStream_t s )
     {
-        k_knn<<<( c.n + kKnnBlock - 1 ) / kKnnBlock, kKnnBlock, 0, s>>>( c );
+        APO2_LAUNCH( "k_knn", s, k_knn<<<( c.n + kKnnBlock - 1 ) / kKnnBlock, kKnnBlock, 0, s>>>( c ) );
     }
 
     void launch_cells( const CellContext & c, cudaStream_t s )
     {
-        k_cells<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c );
+        APO2_LAUNCH( "k_cells", s, k_cells<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c ) );
     }
 
     void launch_tasks( const CellContext & c, uint32_t * tasks, uint32_t * count, cudaStream_t s )
     {
         cudaMemsetAsync( count, 0, sizeof( uint32_t ), s );
-        k_tasks<<<( c.n + 255 ) / 256, 256, 0, s>>>( c.status, c.n, tasks, count );
+        APO2_LAUNCH( "k_tasks", s, k_tasks<<<( c.n + 255 ) / 256, 256, 0, s>>>( c.status, c.n, tasks, count ) );
     }
 
     void launch_vertex_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s )
     {
-        k_vertex_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, tasks, count );
+        APO2_LAUNCH( "k_vertex_validation", s, k_vertex_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, tasks, count ) );
     }
 
-    void launch_edge_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s )
+    void launch_edge_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s,
+                                 SearchProof proof )
     {
-        k_edge_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, tasks, count );
+        APO2_LAUNCH( "k_edge_validation", s, k_edge_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, tasks, count, proof ) );
     }
 
     void launch_bisector_validation( const CellContext & c, cudaStream_t s )
     {
-        k_bisector_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( true ), s>>>( c );
+        APO2_LAUNCH( "k_bisector_validation", s, k_bisector_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( true ), s>>>( c ) );
     }
 
     void launch_output( const CellContext & c, const OutputBuffers & o, cudaStream_t s )
     {
         const uint32_t blocks = std::max( 1u, std::min<uint32_t>( ( c.n + 7 ) / 8, 148 * 16 ) );
-        k_count_owned<<<blocks, 256, 0, s>>>( c, o.vcount, o.ccount );
+        APO2_LAUNCH( "k_count_owned", s, k_count_owned<<<blocks, 256, 0, s>>>( c, o.vcount, o.ccount ) );
         const uint32_t tiles = std::max( 1u, ( c.n + kScanTile - 1 ) / kScanTile );
         scan_exclusive( o.vcount, c.n, o.tile_sums, o.totals + 0, s );
         scan_exclusive( o.ccount, c.n, o.tile_sums + tiles, o.totals + 1, s );
-        k_write_owned<<<blocks, 256, 0, s>>>( c, o.vcount, o.ccount, o.vpos, o.vids, o.vcap, o.cpos, o.cids, o.ccap );
+        APO2_LAUNCH( "k_write_owned", s, k_write_owned<<<blocks, 256, 0, s>>>( c, o.vcount, o.ccount, o.vpos, o.vids, o.vcap, o.cpos, o.cids, o.ccap ) );
     }
 } // namespace apo2

@@ -38,14 +38,69 @@ namespace apo2
         uint4 *          vertices    = nullptr; // n * 152 records (j, k, l, type | status << 8)
         uint4 *          edges       = nullptr; // n * 264 records (j, k, vertex count, status)
         uint32_t *       error       = nullptr;
+        const Scene *    scene       = nullptr; // bounds and radius range of the sites
     };
 
+    // Position of a stored vertex: root `type` of quadrisector(si, sj, sk, sl) with the
+    // sorted ids (topology_update.inl:104-111).
+    __device__ __forceinline__ double4 solve_vertex( const CellContext & c, double4 si, uint4 r )
+    {
+        double4 x[ 2 ] = { make_double4( 0, 0, 0, 0 ), make_double4( 0, 0, 0, 0 ) };
+        quadrisector( si, c.sites[ r.x ], c.sites[ r.y ], c.sites[ r.z ], x[ 0 ], x[ 1 ] );
+        return ( r.w & 0xffu ) ? x[ 1 ] : x[ 0 ];
+    }
+
+    // ---------------------------------------------------------------------------------
+    // Reach of an edge search. A site j contributes to edge (k, l) of cell i only through a
+    // root x that passes the emptiness test against the cell's neighbours, i.e. a point of
+    // the edge's arc inside the current cell, whose empty-sphere radius w(x) is at most the
+    // largest radius over the arc: its vertices and, on an elliptic trisector, an apex that
+    // may lie on the arc (the cell certificate of the reference rests on the same bound,
+    // algorithm.inl:186-190, topology_update.inl:595-653). Then
+    //     |c_j - c_i| <= |c_j - x| + |x - c_i| = 2 w(x) + r_i + r_j,
+    // so the search may skip every BVH node and leaf outside that ball: the leaves it
+    // visits are a subsequence of the reference's, in the same order, and every site that
+    // could contribute is among them, so the first contributor found is the same.
+    // ---------------------------------------------------------------------------------
+    __device__ __forceinline__ bool vertex_on_edge( uint4 r, uint32_t k, uint32_t l )
+    {
+        return ( r.x == k || r.y == k || r.z == k ) && ( r.x == l || r.y == l || r.z == l );
+    }
+
+    // An apex (trisector root in the plane of the centres) counts unless a neighbour other
+    // than k, l clearly intersects its sphere (IEEE double distance, relative margin 1e-4).
+    __device__ __forceinline__ bool clearly_outside( double4 site, double4 apex )
+    {
+        const double dx = site.x - apex.x, dy = site.y - apex.y, dz = site.z - apex.z;
+        const double d  = __dsqrt_rn( __dadd_rn( __dadd_rn( __dmul_rn( dx, dx ), __dmul_rn( dy, dy ) ), __dmul_rn( dz, dz ) ) );
+        const double pen = ( site.w + apex.w ) - d;
+        return pen > 1e-4 * ( site.w + fabs( apex.w ) ) + 1e-6;
+    }
+
+    // Radius of the ball around c_i that holds every possible contributor, with margins.
+    __device__ __forceinline__ float reach_radius( double wmax, double ri, double rmax )
+    {
+        const double r = 2.0 * wmax * 1.01 + ri + rmax + 1e-3 * ( 1.0 + wmax );
+        return float( r ) * 1.0001f + 1e-3f;
+    }
     void configure_cell_kernels();
     void launch_knn( const CellContext & c, cudaStream_t s );
     void launch_cells( const CellContext & c, cudaStream_t s );
     void launch_tasks( const CellContext & c, uint32_t * tasks, uint32_t * count, cudaStream_t s );
     void launch_vertex_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s );
-    void launch_edge_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s );
+    constexpr uint32_t kMaybeWords = ( kMaxEdges + 31 ) / 32; // 9 words of edge bits per task
+    constexpr uint32_t kNbrCap     = 64;                      // neighbour slots per task cell
+
+    // What the edge-parallel search proved, handed to the exact pass of the same cells.
+    struct SearchProof
+    {
+        const uint32_t * slots      = nullptr; // task index of each listed cell
+        const uint32_t * maybe_bits = nullptr; // per task, bit e: edge e may have a contributor
+        const uint32_t * nbr        = nullptr; // per task, the sorted neighbour ids searched against
+        const uint32_t * nbr_count  = nullptr;
+    };
+    void launch_edge_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s,
+                                 SearchProof proof = SearchProof {} );
     void launch_bisector_validation( const CellContext & c, cudaStream_t s );
 
     // Output extraction: per-cell owned counts, exclusive scans (totals[0] vertices,
@@ -64,4 +119,33 @@ namespace apo2
     };
     size_t output_scan_scratch_words( uint32_t n );
     void   launch_output( const CellContext & c, const OutputBuffers & o, cudaStream_t s );
+
+    // Exclusive scan of n u32 values in place; the total goes to *total. `sums` holds
+    // output_scan_scratch_words(n) words.
+    void scan_exclusive( uint32_t * data, uint32_t n, uint32_t * sums, uint64_t * total, cudaStream_t s );
+
+    // Edge-parallel edge validation with an exact per-cell fallback (speculate.cu).
+    struct SpecBuffers
+    {
+        uint32_t * nbr          = nullptr; // per task: sorted unique neighbour ids (64 slots)
+        uint32_t * nbr_count    = nullptr;
+        uint32_t * item_count   = nullptr; // per task: edges to search; scanned into item_offset
+        uint32_t * item_offset  = nullptr;
+        uint32_t * cell_flag    = nullptr; // 1: a contributor was found, 2: neighbour list too long
+        uint32_t * exact_tasks  = nullptr; // cells re-run by the exact warp algorithm
+        uint32_t * exact_slot   = nullptr; // their task index (row of maybe_bits)
+        uint32_t * exact_count  = nullptr;
+        uint32_t * maybe_bits   = nullptr; // per task, bit e: edge e may have a contributor
+        uint64_t * item_total   = nullptr;
+        uint64_t * item_counter = nullptr;
+        uint32_t * scan_sums    = nullptr;
+        uint2 *    heavy        = nullptr; // (task, edge) searches handed to whole warps
+        uint32_t * heavy_count  = nullptr;
+        uint32_t * heavy_next   = nullptr;
+        uint32_t   heavy_cap    = 0;
+    };
+    size_t spec_bytes( uint32_t n );
+    void   spec_carve( SpecBuffers & b, void * base, uint32_t n );
+    void   launch_edge_validation_speculative( const CellContext & c, const uint32_t * tasks, const uint32_t * task_count,
+                                               const SpecBuffers & b, cudaStream_t s );
 } // namespace apo2

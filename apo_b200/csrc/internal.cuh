@@ -11,8 +11,37 @@
 
 #include "geometry.cuh"
 
+// Launches kernel `name` on stream `s` through the launch observer.
+#define APO2_LAUNCH( name, s, ... )             \
+    do                                          \
+    {                                           \
+        ::apo2::observe( name, s, false );      \
+        __VA_ARGS__;                            \
+        ::apo2::observe( name, s, true );       \
+    } while ( 0 )
+
 namespace apo2
 {
+    // Launch observer: the C ABI installs it (per thread) to count the kernels of a build and,
+    // when stage timing is on, to bracket each launch with CUDA events.
+    using LaunchHook = void ( * )( const char * name, cudaStream_t s, bool after, void * ctx );
+    struct LaunchObserver
+    {
+        LaunchHook hook = nullptr;
+        void *     ctx  = nullptr;
+    };
+    inline LaunchObserver & launch_observer()
+    {
+        static thread_local LaunchObserver o;
+        return o;
+    }
+    inline void observe( const char * name, cudaStream_t s, bool after )
+    {
+        const LaunchObserver & o = launch_observer();
+        if ( o.hook )
+            o.hook( name, s, after, o.ctx );
+    }
+
     constexpr uint32_t kNone = 0xffffffffu;
 
     // Per-cell capacities of the reference (apo/include/apo/gpu/algorithm.inl:25-30).

@@ -389,11 +389,11 @@ namespace apo2
     {
         const uint32_t grid = std::min<uint32_t>( partial_count, blocks_for( n, kBoundsBlock ) );
         if ( is_f64 )
-            k_bounds<double4><<<grid, kBoundsBlock, 0, s>>>( static_cast<const double4 *>( input ), n, copy, partials,
-                                                             counter, scene, artificial );
+            APO2_LAUNCH( "k_bounds", s, k_bounds<double4><<<grid, kBoundsBlock, 0, s>>>( static_cast<const double4 *>( input ), n, copy, partials,
+                                                             counter, scene, artificial ) );
         else
-            k_bounds<float4><<<grid, kBoundsBlock, 0, s>>>( static_cast<const float4 *>( input ), n, copy, partials,
-                                                            counter, scene, artificial );
+            APO2_LAUNCH( "k_bounds", s, k_bounds<float4><<<grid, kBoundsBlock, 0, s>>>( static_cast<const float4 *>( input ), n, copy, partials,
+                                                            counter, scene, artificial ) );
     }
 
     size_t bounds_partial_bytes( uint32_t count ) { return sizeof( BoundsPartial ) * count; }
@@ -401,15 +401,15 @@ namespace apo2
     void launch_tree( const Tree & t, uint32_t n, const double4 * input, const Scene * scene, SortScratch & sort,
                       cudaStream_t s )
     {
-        k_morton<<<blocks_for( n, 256 ), 256, 0, s>>>( input, scene, n, t.codes, t.indices );
+        APO2_LAUNCH( "k_morton", s, k_morton<<<blocks_for( n, 256 ), 256, 0, s>>>( input, scene, n, t.codes, t.indices ) );
         radix_sort_pairs( t.codes, t.indices, n, sort, s );
-        k_leaves<<<blocks_for( n, 256 ), 256, 0, s>>>( input, t.indices, n, t.sites, t.sites_f, t.boxes, t.left, t.right );
+        APO2_LAUNCH( "k_leaves", s, k_leaves<<<blocks_for( n, 256 ), 256, 0, s>>>( input, t.indices, n, t.sites, t.sites_f, t.boxes, t.left, t.right ) );
         if ( n > 1 )
         {
-            k_karras<<<blocks_for( n - 1, 256 ), 256, 0, s>>>( t.codes, n, t.parent, t.left, t.right );
+            APO2_LAUNCH( "k_karras", s, k_karras<<<blocks_for( n - 1, 256 ), 256, 0, s>>>( t.codes, n, t.parent, t.left, t.right ) );
             cudaMemsetAsync( t.arrivals, 0, sizeof( uint32_t ) * ( n - 1 ), s );
-            k_refit<<<blocks_for( n, 256 ), 256, 0, s>>>( n, t.arrivals, t.parent, t.left, t.right, t.boxes, t.sizes );
-            k_pack<<<blocks_for( n - 1, 256 ), 256, 0, s>>>( n, t.left, t.right, t.boxes, t.nodes );
+            APO2_LAUNCH( "k_refit", s, k_refit<<<blocks_for( n, 256 ), 256, 0, s>>>( n, t.arrivals, t.parent, t.left, t.right, t.boxes, t.sizes ) );
+            APO2_LAUNCH( "k_pack", s, k_pack<<<blocks_for( n - 1, 256 ), 256, 0, s>>>( n, t.left, t.right, t.boxes, t.nodes ) );
         }
     }
 
@@ -417,14 +417,14 @@ namespace apo2
                           int32_t * parent, int32_t * left, int32_t * right, float4 * boxes, uint32_t * sizes,
                           uint32_t * arrivals, SortScratch & sort, cudaStream_t s )
     {
-        k_morton_f32<<<blocks_for( n, 256 ), 256, 0, s>>>( sites, lo, scale, n, codes, indices );
+        APO2_LAUNCH( "k_morton_f32", s, k_morton_f32<<<blocks_for( n, 256 ), 256, 0, s>>>( sites, lo, scale, n, codes, indices ) );
         radix_sort_pairs( codes, indices, n, sort, s );
-        k_leaves_f32<<<blocks_for( n, 256 ), 256, 0, s>>>( sites, indices, n, boxes, left, right );
+        APO2_LAUNCH( "k_leaves_f32", s, k_leaves_f32<<<blocks_for( n, 256 ), 256, 0, s>>>( sites, indices, n, boxes, left, right ) );
         if ( n > 1 )
         {
-            k_karras<<<blocks_for( n - 1, 256 ), 256, 0, s>>>( codes, n, parent, left, right );
+            APO2_LAUNCH( "k_karras", s, k_karras<<<blocks_for( n - 1, 256 ), 256, 0, s>>>( codes, n, parent, left, right ) );
             cudaMemsetAsync( arrivals, 0, sizeof( uint32_t ) * ( n - 1 ), s );
-            k_refit<<<blocks_for( n, 256 ), 256, 0, s>>>( n, arrivals, parent, left, right, boxes, sizes );
+            APO2_LAUNCH( "k_refit", s, k_refit<<<blocks_for( n, 256 ), 256, 0, s>>>( n, arrivals, parent, left, right, boxes, sizes ) );
         }
     }
 } // namespace apo2

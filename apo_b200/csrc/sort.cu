@@ -271,8 +271,8 @@ namespace apo2
         cudaMemsetAsync( s.histograms, 0, sizeof( uint32_t ) * kPasses * kRadix, stream );
         cudaMemsetAsync( s.tile_counter, 0, sizeof( uint32_t ) * kPasses, stream );
         const uint32_t hist_blocks = std::min<uint32_t>( 296, ( n + kSortThreads * 8 - 1 ) / ( kSortThreads * 8 ) );
-        k_digit_histograms<<<std::max( 1u, hist_blocks ), kSortThreads, 0, stream>>>( keys, n, s.histograms );
-        k_scan_histograms<<<kPasses, kRadix, 0, stream>>>( s.histograms );
+        APO2_LAUNCH( "k_digit_histograms", stream, k_digit_histograms<<<std::max( 1u, hist_blocks ), kSortThreads, 0, stream>>>( keys, n, s.histograms ) );
+        APO2_LAUNCH( "k_scan_histograms", stream, k_scan_histograms<<<kPasses, kRadix, 0, stream>>>( s.histograms ) );
 
         uint64_t * kin = keys;
         uint32_t * vin = values;
@@ -281,8 +281,8 @@ namespace apo2
         for ( uint32_t p = 0; p < kPasses; p++ )
         {
             cudaMemsetAsync( s.lookback, 0, sizeof( uint32_t ) * size_t( tiles ) * kRadix, stream );
-            k_onesweep<<<tiles, kSortThreads, sizeof( OnesweepShared ), stream>>>(
-                kin, vin, kout, vout, n, p * kRadixBits, s.histograms + p * kRadix, s.lookback, s.tile_counter + p, s.error );
+            APO2_LAUNCH( "k_onesweep", stream, k_onesweep<<<tiles, kSortThreads, sizeof( OnesweepShared ), stream>>>(
+                kin, vin, kout, vout, n, p * kRadixBits, s.histograms + p * kRadix, s.lookback, s.tile_counter + p, s.error ) );
             std::swap( kin, kout );
             std::swap( vin, vout );
         }

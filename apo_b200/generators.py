@@ -100,3 +100,40 @@ def uniform_random(count: int, side: float, rmin: float, rmax: float, seed: int)
     out[:, :3] = rng.uniform(0.0, side, size=(count, 3))
     out[:, 3] = rng.uniform(rmin, rmax, size=count)
     return out
+
+
+def protein_chains(chains: int = 2000, atoms_per_chain: int = 500, density: float = 0.01, seed: int = 1) -> np.ndarray:
+    """Protein-like packing: self-avoiding random-walk chains (bond 1.53 A, angle 109.5 +/- 10
+    degrees, uniform torsion, vdW radii {1.20: 40%, 1.70: 32%, 1.55: 14%, 1.52: 13%, 1.80: 1%},
+    non-bonded overlap above 0.5 A rejected) at `density` atoms per A^3. Generated by the
+    library's C++ generator (apo2_generate_chains)."""
+    import ctypes
+    from . import load_library, _check
+    out = np.zeros((chains * atoms_per_chain, 4), dtype=np.float32)
+    _check(load_library().apo2_generate_chains(chains, atoms_per_chain, density, seed, out.ctypes.data))
+    return out
+
+
+def lattice(side: int = 126, variant: str = "A", seed: int = 1) -> np.ndarray:
+    """Near-degenerate stress set: side^3 sites on a cubic lattice jittered by N(0, 1e-4).
+    Variant A: spacing 2.0, radii 1.0 + U(0, 1e-5) (tangent spheres). Variant B: spacing 3.0,
+    radii log-normal(0, 0.5) clipped to [0.2, 3.0]."""
+    rng = np.random.default_rng(seed)
+    spacing = 2.0 if variant == "A" else 3.0
+    g = np.arange(side, dtype=np.float64) * spacing
+    xyz = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+    xyz = xyz + rng.normal(0.0, 1e-4, size=xyz.shape)
+    if variant == "A":
+        r = 1.0 + rng.uniform(0.0, 1e-5, size=xyz.shape[0])
+    else:
+        r = np.clip(rng.lognormal(0.0, 0.5, size=xyz.shape[0]), 0.2, 3.0)
+    out = np.empty((xyz.shape[0], 4), dtype=np.float32)
+    out[:, :3] = xyz
+    out[:, 3] = r
+    return out
+
+
+def batch_sizes(count: int = 4096, lo: int = 200, hi: int = 50000, seed: int = 1) -> np.ndarray:
+    """Diagram sizes log-uniform in [lo, hi] (batched workload)."""
+    rng = np.random.default_rng(seed)
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), size=count)).astype(np.int64)

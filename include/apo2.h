@@ -68,7 +68,9 @@ typedef struct apo2_options
     uint32_t max_iterations;       /* validation rounds; 0 = 10 (algorithm.inl:1554) */
     uint32_t device;               /* CUDA device ordinal */
     uint32_t stage_timing;         /* 1 = record per-stage CUDA-event times (apo2_stats) */
-    uint32_t reserved[ 11 ];
+    uint32_t edge_search;          /* 0 = edge-parallel search with exact per-cell fallback (default),
+                                      1 = warp-per-cell edge validation only; both give the same result */
+    uint32_t reserved[ 10 ];
 } apo2_options;
 
 /* Per-build statistics, the counterpart of AlgorithmGPU::Sample (algorithm.cuh:18-27). */
@@ -78,8 +80,9 @@ typedef struct apo2_stats
     uint32_t buried;               /* cells of sites inside another site */
     uint32_t certified_after_knn;  /* cells certified by the kNN security radius */
     uint32_t validation_rounds;    /* vertex+edge validation rounds that had work */
-    uint32_t error_flags;          /* capacity flags (1 vertex, 2 edge, 4 new edge, 8 bisector, 16 stack) */
-    uint32_t reserved0;
+    uint32_t error_flags;          /* capacity flags (1 vertex, 2 edge, 4 new edge, 8 bisector, 16 stack,
+                                      32 sort look-back, 64 walk or restart bound) */
+    uint32_t kernel_launches;      /* kernels launched by the last build (+ extraction) */
     uint64_t vertex_records;       /* sum of per-cell vertex counts */
     uint64_t edge_records;         /* sum of per-cell edge counts */
     uint64_t output_vertices;      /* vertices owned by their smallest site (toHost) */
@@ -167,6 +170,11 @@ apo2_status apo2_debug_array( apo2_handle * h, const char * name, void * dst, ui
 
 apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats );
 
+/* Kernel launches of the last build as JSON text: {"launches": L, "timed": bool, "kernels":
+ * {"name": [count, total_ms], ...}} (times only with stage_timing). With json == NULL only
+ * *length is set. */
+apo2_status apo2_kernel_profile( apo2_handle * h, char * json, uint64_t capacity, uint64_t * length );
+
 apo2_status apo2_destroy( apo2_handle * h );
 
 /* One-call forms of the reference's free functions (apo/include/apo/gpu/algorithm.hpp:58-59):
@@ -193,6 +201,12 @@ apo2_status apo2_lbvh_build( const float * sites_xyzr, uint32_t n, const float s
  * keys/values are sorted in place; `scratch` must hold apo2_radix_sort_scratch_bytes(n). */
 uint64_t    apo2_radix_sort_scratch_bytes( uint32_t n );
 apo2_status apo2_radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t n, void * scratch, void * stream );
+
+/* Seeded protein-like site set (host): `chains` self-avoiding random-walk chains of
+ * `atoms_per_chain` atoms (bond 1.53 A, bond angle 109.5 +/- 10 deg, uniform torsion, van der
+ * Waals radii mix) in a cube of `density` atoms per A^3, written as float (x, y, z, r).
+ * Stand-in for the reference's PDB inputs (app/common/samples.cpp:10-61), which need chemfiles. */
+apo2_status apo2_generate_chains( uint32_t chains, uint32_t atoms_per_chain, double density, uint64_t seed, float * out_xyzr );
 
 #ifdef __cplusplus
 }

@@ -406,8 +406,22 @@ namespace
         kFlagStack     = 16,
     };
 
+    // Work counters (for profiling the restated algorithm; no effect on results).
+    enum Counter
+    {
+        cEdgeTasks, cEdgeSearched, cEdgeSecurity, cEdgeLeaves, cEdgeCandidates, cEdgeSolves, cEdgeFound, cEdgeCellsChanged,
+        cVertexSearched, cVertexLeaves, cVertexInvalid, cVertexCellsChanged, cBisSearched, cBisLeaves, cBisCandidates,
+        cBisFound, cBisCellsChanged, cEdgeCellsFound, cEdgeCandInBall, cEdgeFoundOutsideBall, cEdgeSolvesInBall, cCounterCount
+    };
+
     struct Context
     {
+        std::vector<uint64_t> counters = std::vector<uint64_t>( cCounterCount, 0 );
+        void count( Counter c, uint64_t v = 1 )
+        {
+#pragma omp atomic
+            counters[ c ] += v;
+        }
         uint32_t             n = 0;
         std::vector<D4>      sites; // n + 6, Morton order then the 6 artificial sites
         std::vector<uint8_t> status;
@@ -427,6 +441,10 @@ namespace
         std::vector<uint32_t> outVerticesId, outClosedId, topoQuad, topoTri, topoBi;
         // flattened stores for inspection
         std::vector<uint32_t> vertexNb, edgeNb, flatVertices, flatEdges;
+        // per searched edge of the edge passes: cell, k, l, leaves reached, candidates, round
+        std::vector<uint32_t> edgeSearchLog;
+        double                rmax = 0.0;
+        int                   round = 0;
         uint32_t              flagsAll = 0;
 
         Box box( uint32_t node ) const
@@ -1189,6 +1207,7 @@ namespace
                     continue;
 
                 // nearest admissible site to the vertex sphere (per-lane BVH walk)
+                ctx.count( cVertexSearched );
                 const Vertex vtx = c.v[ vid ];
                 const F4     fc  = toFloat( current[ lane ] );
                 struct Entry { uint32_t node; float d; };
@@ -1221,6 +1240,7 @@ namespace
                     }
                     if ( node >= n - 1 && node < 2 * n - 1 )
                     {
+                        ctx.count( cVertexLeaves );
                         const uint32_t j = node - ( n - 1 );
                         if ( j != i && j != vtx.j && j != vtx.k && j != vtx.l && ctx.status[ j ] != kBuried
                              && !w.known( j ) )
@@ -1268,6 +1288,9 @@ namespace
             }
             if ( changed )
             {
+                ctx.count( cVertexInvalid, uint64_t( __builtin_popcount( changed ) ) );
+                if ( restarts == 0 )
+                    ctx.count( cVertexCellsChanged );
                 vs = 0;
                 restarts++;
             }
@@ -1311,7 +1334,7 @@ namespace
         CellWork w { ctx, i, ctx.sites[ i ], pass, ctx.flags[ i ] };
         const D4 si  = w.si;
         const F4 fsi = toFloat( si );
-        bool     didChange = false;
+        bool     didChange = false, anyFound = false;
 
         const uint32_t stepNb = pass.en / 32 + 1;
         for ( uint32_t es = 0; es < stepNb; es++ )
@@ -1371,10 +1394,49 @@ namespace
                     pass.e[ eid[ lane ] ].status = 1;
                     needSearch[ lane ]           = false;
                 }
+                if ( eid[ lane ] < pass.en )
+                    ctx.count( cEdgeTasks );
+                if ( eid[ lane ] < pass.en && inSecurity )
+                    ctx.count( cEdgeSecurity );
                 if ( !needSearch[ lane ] )
                     continue;
+                ctx.count( cEdgeSearched );
 
-                // first admissible contributor inside the bounding volume (per-lane walk)
+                // (profiling only) radius bound of the edge arc: its vertices and, for an
+                // elliptic trisector, its apexes
+                double wEdge = 0.0;
+                for ( uint32_t v = 0; v < stored.vn; v++ )
+                {
+                    const Vertex & vx = stored.v[ v ];
+                    const bool hasK = vx.j == k || vx.k == k || vx.l == k;
+                    const bool hasL = vx.j == l || vx.k == l || vx.l == l;
+                    if ( hasK && hasL )
+                        wEdge = dmax( wEdge, w.vertexPosition( vx ).w );
+                }
+                if ( edgeType == 2 || pass.e[ eid[ lane ] ].vertexNb == kNone )
+                {
+                    // an apex counts when it may lie on the cell's arc: no neighbour other
+                    // than k, l clearly intersects its sphere
+                    for ( int a = 0; a < 2; a++ )
+                    {
+                        bool clearlyOut = false;
+                        for ( uint32_t e2 = 0; e2 < pass.en && !clearlyOut; e2++ )
+                            for ( uint32_t u : { pass.e[ e2 ].j, pass.e[ e2 ].k } )
+                            {
+                                if ( u == k || u == l )
+                                    continue;
+                                const D4     su  = ctx.sites[ u ];
+                                const double d   = std::sqrt( dot( sub( xyz( su ), xyz( ev[ a ] ) ), sub( xyz( su ), xyz( ev[ a ] ) ) ) );
+                                const double pen = ( su.w + ev[ a ].w ) - d;
+                                if ( pen > 1e-4 * ( su.w + std::fabs( ev[ a ].w ) ) + 1e-6 )
+                                    clearlyOut = true;
+                            }
+                        if ( !clearlyOut )
+                            wEdge = dmax( wEdge, ev[ a ].w );
+                    }
+                }
+                const double ballR = 2.0 * wEdge * 1.01 + si.w + ctx.rmax + 1e-3;
+                uint32_t logLeaves = 0, logCandidates = 0, logInBall = 0;
                 uint32_t stack[ 64 ];
                 int      sp = 0;
                 uint32_t node = 0;
@@ -1413,6 +1475,8 @@ namespace
                     }
                     if ( node >= n - 1 && node < 2 * n - 1 )
                     {
+                        ctx.count( cEdgeLeaves );
+                        logLeaves++;
                         const uint32_t j   = node - ( n - 1 );
                         bool           can = j != i && j != k && j != l && ctx.status[ j ] != kBuried;
                         D4             sj {};
@@ -1425,11 +1489,24 @@ namespace
                                 can = can && double( dot( n1, sub( xyz( fj ), pp1 ) ) ) < -sj.w
                                       && double( dot( n2, sub( xyz( fj ), pp2 ) ) ) < -sj.w;
                         }
+                        bool inBall = false;
+                        if ( can )
+                        {
+                            ctx.count( cEdgeCandidates );
+                            logCandidates++;
+                            inBall = length( sub( xyz( sj ), xyz( si ) ) ) <= ballR;
+                            if ( inBall )
+                            {
+                                ctx.count( cEdgeCandInBall );
+                                logInBall++;
+                            }
+                        }
                         can = can && !w.known( j );
                         uint8_t mask = 0;
                         D4      x[ 2 ] = {};
                         if ( can )
                         {
+                            ctx.count( cEdgeSolves );
                             mask = quadrisector( si, sj, sk, sl, x[ 0 ], x[ 1 ] );
                             if ( mask != 3 )
                                 mask = 0;
@@ -1442,8 +1519,12 @@ namespace
                             if ( !w.predicate( x[ nv ], k, l ) )
                                 valid &= uint8_t( ~( 1u << nv ) );
                         }
+                        if ( can && inBall )
+                            ctx.count( cEdgeSolvesInBall );
                         if ( valid )
                         {
+                            if ( !inBall )
+                                ctx.count( cEdgeFoundOutsideBall );
                             found[ lane ] = j;
                             cont          = false;
                         }
@@ -1456,8 +1537,20 @@ namespace
                             node = stack[ --sp ];
                     }
                 }
+#pragma omp critical( edge_log )
+                {
+                    uint32_t b[ 4 ];
+                    std::memcpy( b, &bsph, 16 );
+                    ctx.edgeSearchLog.insert( ctx.edgeSearchLog.end(),
+                                              { i, k, l, logLeaves, logCandidates, uint32_t( ctx.round ), edgeType, b[ 0 ], b[ 1 ], b[ 2 ], b[ 3 ], logInBall, uint32_t( std::min( ballR, 4e9 ) ) } );
+                }
                 if ( found[ lane ] == kNone )
                     pass.e[ eid[ lane ] ].status = 1;
+                else
+                {
+                    ctx.count( cEdgeFound );
+                    anyFound = true;
+                }
             }
             for ( int lane = 31; lane >= 0; lane-- )
             {
@@ -1472,6 +1565,10 @@ namespace
                     es = 0;
             }
         }
+        if ( didChange )
+            ctx.count( cEdgeCellsChanged );
+        if ( anyFound )
+            ctx.count( cEdgeCellsFound );
         appendPassVertices( stored, stored.v, stored.vn, pass );
         ctx.status[ i ] = didChange ? 0 : 1;
     }
@@ -1559,6 +1656,7 @@ namespace
                 }
                 if ( !needSearch )
                     continue;
+                ctx.count( cBisSearched );
                 const F3    center = scale( add( fci, fck ), .5f );
                 const float radius = length( sub( center, fci ) ) + fmaxf_( fri, frk );
                 const F4    bsph { center.x, center.y, center.z, radius };
@@ -1593,6 +1691,7 @@ namespace
                     }
                     if ( node >= n - 1 && node < 2 * n - 1 )
                     {
+                        ctx.count( cBisLeaves );
                         const uint32_t j   = node - ( n - 1 );
                         bool           can = j != i && j != bisector;
                         D4             sj {};
@@ -1610,6 +1709,8 @@ namespace
                                 can              = ( d + fj.w ) < cylinderRadius;
                             }
                         }
+                        if ( can )
+                            ctx.count( cBisCandidates );
                         can = can && !w.known( j );
                         D4 vtx {};
                         if ( can )
@@ -1637,6 +1738,8 @@ namespace
                 }
                 if ( found[ lane ] == kNone )
                     bis[ bid ] = kNone;
+                else
+                    ctx.count( cBisFound );
             }
             for ( int lane = 31; lane >= 0; lane-- )
             {
@@ -1651,6 +1754,8 @@ namespace
                     bs = 0;
             }
         }
+        if ( didChange )
+            ctx.count( cBisCellsChanged );
         appendPassVertices( stored, stored.v, stored.vn, pass );
         ctx.status[ i ] = didChange ? 0 : 1;
     }
@@ -1688,6 +1793,7 @@ namespace
             mx[ 1 ]    = std::max( mx[ 1 ], s.y + s.w );
             mx[ 2 ]    = std::max( mx[ 2 ], s.z + s.w );
             minRadius  = std::min( minRadius, s.w );
+            ctx.rmax   = std::max( ctx.rmax, s.w );
         }
         buildLbvh( ctx, input, mn, mx );
 
@@ -1733,6 +1839,7 @@ namespace
             for ( int iteration = 0; iteration < 10 && !tasks.empty(); iteration++ )
             {
                 parallelFor( uint32_t( tasks.size() ), threads, [ & ]( uint32_t t ) { vertexValidation( ctx, tasks[ t ] ); } );
+                ctx.round = iteration;
                 parallelFor( uint32_t( tasks.size() ), threads, [ & ]( uint32_t t ) { edgeValidation( ctx, tasks[ t ] ); } );
                 tasks.clear();
                 for ( uint32_t i = 0; i < n; i++ )
@@ -1919,6 +2026,8 @@ uint64_t oracle_get( const oracle_run * r, const char * name, const void ** data
     ORACLE_ARRAY( "topo_quad", c.topoQuad )
     ORACLE_ARRAY( "topo_tri", c.topoTri )
     ORACLE_ARRAY( "topo_bi", c.topoBi )
+    ORACLE_ARRAY( "counters", c.counters )
+    ORACLE_ARRAY( "edge_search_log", c.edgeSearchLog )
 #undef ORACLE_ARRAY
     if ( key == "sites_sorted" )
     {

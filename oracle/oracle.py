@@ -23,8 +23,14 @@ _ARRAYS = {
     "edge_nb": np.uint32, "vertices": np.uint32, "edges": np.uint32,
     "out_vertices": np.float64, "out_vertices_id": np.uint32, "out_closed": np.float64,
     "out_closed_id": np.uint32, "topo_quad": np.uint32, "topo_tri": np.uint32,
-    "topo_bi": np.uint32,
+    "topo_bi": np.uint32, "counters": np.uint64, "edge_search_log": np.uint32,
 }
+
+COUNTERS = ["edge_tasks", "edge_searched", "edge_security", "edge_leaves", "edge_candidates", "edge_solves",
+            "edge_found", "edge_cells_changed", "vertex_searched", "vertex_leaves", "vertex_invalid",
+            "vertex_cells_changed", "bisector_searched", "bisector_leaves", "bisector_candidates", "bisector_found",
+            "bisector_cells_changed", "edge_cells_found", "edge_candidates_in_ball", "edge_found_outside_ball",
+            "edge_solves_in_ball"]
 
 _lib = None
 

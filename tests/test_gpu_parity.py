@@ -185,3 +185,18 @@ def test_invalid_arguments(apo):
     opt.k = 64
     two = np.zeros(8, dtype=np.float32)
     assert lib.apo2_create(two.ctypes.data, 2, 0, 0, ctypes.byref(opt), ctypes.byref(h)) == apo.APO2_ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("case", ["uni2k", "lognormal"])
+def test_edge_search_modes_agree(apo, case):
+    """The edge-parallel edge validation and the warp-per-cell one leave identical stores."""
+    from apo_b200 import generators as g
+    sites = H.sites_for(case) if case != "lognormal" else g.lognormal_cloud(30000, 400.0 * (30000 / 5e6) ** (1 / 3), 21)
+    stores = []
+    for mode in (0, 1):
+        algo = apo.AlgorithmGPU(sites, edge_search=mode)
+        algo.build()
+        stores.append({name: algo.debug_array(name) for name in ("status", "vertex_nb", "edge_nb", "vertices", "edges")})
+        algo.close()
+    for name in stores[0]:
+        assert np.array_equal(stores[0][name], stores[1][name]), name
