@@ -90,6 +90,7 @@ SIGNATURES = {
     "apo2_lbvh_build": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "apo2_radix_sort_scratch_bytes": (_U64, [_U32]),
     "apo2_radix_sort_pairs": (_I, [_P, _P, _U32, _P, _P]),
+    "apo2_radix_sort_pairs_static": (_I, [_P, _P, _U32, _P]),
     "apo2_generate_chains": (_I, [_U32, _U32, ctypes.c_double, _U64, _P]),
 }
 
