@@ -23,7 +23,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libapo2.so")
+LIB_PATH = os.environ.get("APO2_LIBRARY") or os.path.join(HERE, "libapo2.so")
 
 APO2_OK, APO2_ERR_INVALID_ARG, APO2_ERR_CAPACITY, APO2_ERR_ITER_LIMIT, APO2_ERR_CUDA = 0, 1, 2, 3, 4
 APO2_ERR_NOT_BUILT, APO2_ERR_OUT_OF_MEMORY, APO2_ERR_TOO_LARGE = 5, 6, 7

@@ -769,7 +769,7 @@ namespace apo2
         __syncwarp();
     }
 
-    __global__ void __launch_bounds__( kCellBlock ) k_cells( CellContext c )
+    __global__ void __launch_bounds__( kCellBlock, 4 ) k_cells( CellContext c )
     {
         extern __shared__ __align__( 16 ) unsigned char smem[];
         const uint32_t warp  = threadIdx.x >> 5;
@@ -819,7 +819,7 @@ namespace apo2
     // -----------------------------------------------------------------------------------
     // Vertex validation (algorithm.inl:208-476)
     // -----------------------------------------------------------------------------------
-    __global__ void __launch_bounds__( kCellBlock ) k_vertex_validation( CellContext c, const uint32_t * __restrict__ tasks,
+    __global__ void __launch_bounds__( kCellBlock, 4 ) k_vertex_validation( CellContext c, const uint32_t * __restrict__ tasks,
                                                                         const uint32_t * __restrict__ task_count )
     {
         extern __shared__ __align__( 16 ) unsigned char smem[];
@@ -909,7 +909,7 @@ namespace apo2
                     {
                         const uint32_t t2 = highest( cm );
                         cm &= ~( 1u << t2 );
-                        const uint32_t tj    = __shfl_sync( kFull, j, t2 );
+                        const uint32_t tj     = __shfl_sync( kFull, j, t2 );
                         const bool     known2 = is_known( w, tj );
                         if ( lane == t2 )
                             can = !known2;
@@ -976,7 +976,7 @@ namespace apo2
     // while the cell's neighbours still include all of U0 (updates only added some), an edge
     // with no contributor then has none now: its search would find nothing and is skipped.
     // Once a neighbour of U0 has left the cell, every edge is searched again.
-    __global__ void __launch_bounds__( kCellBlock ) k_edge_validation( CellContext c, const uint32_t * __restrict__ tasks,
+    __global__ void __launch_bounds__( kCellBlock, 4 ) k_edge_validation( CellContext c, const uint32_t * __restrict__ tasks,
                                                                       const uint32_t * __restrict__ task_count,
                                                                       SearchProof proof )
     {
@@ -1271,7 +1271,7 @@ namespace apo2
     // -----------------------------------------------------------------------------------
     // Bisector validation (algorithm.inl:859-1233)
     // -----------------------------------------------------------------------------------
-    __global__ void __launch_bounds__( kCellBlock ) k_bisector_validation( CellContext c )
+    __global__ void __launch_bounds__( kCellBlock, 3 ) k_bisector_validation( CellContext c )
     {
         extern __shared__ __align__( 16 ) unsigned char smem[];
         const uint32_t warp  = threadIdx.x >> 5;
@@ -1451,7 +1451,7 @@ namespace apo2
                     uint32_t cm = __ballot_sync( kFull, can );
                     while ( cm )
                     {
-                        const uint32_t t2     = highest( cm );
+                        const uint32_t t2 = highest( cm );
                         cm &= ~( 1u << t2 );
                         const uint32_t tj     = __shfl_sync( kFull, j, t2 );
                         const bool     known2 = is_known( w, tj );

@@ -143,6 +143,10 @@ namespace apo2
         uint32_t * heavy_count  = nullptr;
         uint32_t * heavy_next   = nullptr;
         uint32_t   heavy_cap    = 0;
+        uint2 *    sub          = nullptr; // (heavy item, BVH node) subtrees of long searches
+        uint32_t * sub_count    = nullptr;
+        uint32_t * sub_next     = nullptr;
+        uint32_t   sub_cap      = 0;
     };
     size_t spec_bytes( uint32_t n );
     void   spec_carve( SpecBuffers & b, void * base, uint32_t n );

@@ -22,9 +22,10 @@ namespace apo2
     constexpr uint32_t kSpecBlock     = 128;
     constexpr uint32_t kFlagFound     = 1;
     constexpr uint32_t kFlagOverflow  = 2;
-    constexpr uint32_t kLaneBudget    = 384;  // leaves one lane may visit before the search goes to a warp
+    constexpr uint32_t kLaneBudget    = 128;  // walk steps one lane may take before the search goes to a warp
     constexpr uint32_t kHeavyBlock    = 128;
     constexpr uint32_t kHeavyStack    = 3072; // shared node stack per warp of the cooperative walk
+    constexpr uint32_t kSplitAt       = 192;  // pending subtrees at which a long walk is handed out
 
     __device__ __forceinline__ uint32_t lane_of() { return threadIdx.x & 31; }
 
@@ -271,7 +272,7 @@ namespace apo2
         return false;
     }
 
-    __global__ void __launch_bounds__( kSpecBlock ) k_edge_speculate( CellContext c, const uint32_t * __restrict__ tasks,
+    __global__ void __launch_bounds__( kSpecBlock, 4 ) k_edge_speculate( CellContext c, const uint32_t * __restrict__ tasks,
                                                                       const uint32_t * __restrict__ task_count,
                                                                       SpecBuffers b, uint32_t * error )
     {
@@ -397,14 +398,102 @@ namespace apo2
 
     // Searches that outgrew one lane: the warp walks the tree together, 32 nodes per step
     // from a shared stack. Only whether a contributor exists matters here, which does not
-    // depend on the visit order.
-    __global__ void __launch_bounds__( kHeavyBlock ) k_edge_heavy( CellContext c, const uint32_t * __restrict__ tasks,
-                                                                   SpecBuffers b, uint32_t * error )
+    // depend on the visit order, so a long walk can also be cut into subtrees that other
+    // warps finish (k_edge_heavy spills its stack once it holds kSplitAt nodes; k_edge_heavy_sub
+    // walks each spilled subtree).
+    enum WalkEnd : uint32_t
+    {
+        kWalkDone,
+        kWalkFound,
+        kWalkOverflow,
+        kWalkSplit
+    };
+
+    __device__ uint32_t cooperative_walk( const CellContext & c, const EdgeSearch & s, uint32_t * st, uint32_t & size,
+                                          uint32_t split_at )
+    {
+        const uint32_t lane = lane_of();
+        const uint32_t n    = c.n;
+        while ( size > 0 )
+        {
+            if ( size >= split_at )
+                return kWalkSplit;
+            const uint32_t take = min( size, 32u );
+            uint32_t       node = kNone;
+            if ( lane < take )
+                node = st[ size - take + lane ];
+            size -= take;
+            __syncwarp();
+            bool     hit = false, eL = false, eR = false;
+            uint32_t lc = 0, rc = 0;
+            if ( node != kNone )
+            {
+                if ( node >= n - 1 )
+                    hit = node < 2 * n - 1 && contributes( c, s, node - ( n - 1 ) );
+                else
+                {
+                    Box lb, rb;
+                    load_node( c.nodes, node, lb, rb, lc, rc );
+                    eL = enter_child( s, lb, lb.distance( s.bsph ) );
+                    eR = enter_child( s, rb, rb.distance( s.bsph ) );
+                }
+            }
+            if ( __any_sync( 0xffffffffu, hit ) )
+                return kWalkFound;
+            const uint32_t pushes = uint32_t( eL ) + uint32_t( eR );
+            uint32_t       x      = pushes;
+#pragma unroll
+            for ( int o = 1; o < 32; o <<= 1 )
+            {
+                const uint32_t y = __shfl_up_sync( 0xffffffffu, x, o );
+                if ( lane >= uint32_t( o ) )
+                    x += y;
+            }
+            const uint32_t total = __shfl_sync( 0xffffffffu, x, 31 );
+            uint32_t       off   = x - pushes;
+            if ( size + total > kHeavyStack )
+                return kWalkOverflow;
+            if ( eL )
+                st[ size + off++ ] = lc;
+            if ( eR )
+                st[ size + off ] = rc;
+            size += total;
+            __syncwarp();
+        }
+        return kWalkDone;
+    }
+
+    __device__ __forceinline__ void search_of_heavy( const CellContext & c, const uint32_t * tasks, const SpecBuffers & b,
+                                                     uint2 h, EdgeSearch & s )
+    {
+        s.t           = h.x;
+        s.e           = h.y;
+        s.i           = tasks[ s.t ];
+        const uint4 r = c.edges[ size_t( s.i ) * kMaxEdges + s.e ];
+        s.k           = r.x;
+        s.l           = r.y;
+        s.closed      = r.z == kNone;
+        s.si          = c.sites[ s.i ];
+        s.sk          = c.sites[ s.k ];
+        s.sl          = c.sites[ s.l ];
+        s.nbr         = b.nbr + size_t( s.t ) * kNbrCap;
+        s.nbr_count   = b.nbr_count[ s.t ];
+        setup_edge( c, s, c.known_radii[ s.i ] ); // the lane path already found it needs a search
+    }
+
+    __device__ __forceinline__ void send_to_exact( const SpecBuffers & b, uint32_t t, uint32_t e )
+    {
+        // the exact path decides, searching this edge again
+        atomicOr( &b.maybe_bits[ size_t( t ) * kMaybeWords + ( e >> 5 ) ], 1u << ( e & 31 ) );
+        atomicOr( &b.cell_flag[ t ], kFlagFound );
+    }
+
+    __global__ void __launch_bounds__( kHeavyBlock, 4 ) k_edge_heavy( CellContext c, const uint32_t * __restrict__ tasks,
+                                                                      SpecBuffers b, uint32_t * error )
     {
         __shared__ uint32_t stacks[ kHeavyBlock / 32 ][ kHeavyStack ];
         const uint32_t      warp  = threadIdx.x >> 5, lane = lane_of();
         uint32_t *          st    = stacks[ warp ];
-        const uint32_t      n     = c.n;
         const uint32_t      count = min( *b.heavy_count, b.heavy_cap );
         while ( true )
         {
@@ -423,81 +512,65 @@ namespace apo2
                 continue;
             }
             EdgeSearch s;
-            s.t         = h.x;
-            s.e         = h.y;
-            s.i         = tasks[ s.t ];
-            const uint4 r = c.edges[ size_t( s.i ) * kMaxEdges + s.e ];
-            s.k         = r.x;
-            s.l         = r.y;
-            s.closed    = r.z == kNone;
-            s.si        = c.sites[ s.i ];
-            s.sk        = c.sites[ s.k ];
-            s.sl        = c.sites[ s.l ];
-            s.nbr       = b.nbr + size_t( s.t ) * kNbrCap;
-            s.nbr_count = b.nbr_count[ s.t ];
-            setup_edge( c, s, c.known_radii[ s.i ] ); // the lane path already found it needs a search
-
-            uint32_t size  = 1;
-            bool     found = false, overflow = false;
+            search_of_heavy( c, tasks, b, h, s );
+            uint32_t size = 1;
             if ( lane == 0 )
                 st[ 0 ] = 0;
             __syncwarp();
-            while ( size > 0 && !found && !overflow )
+            const uint32_t end = cooperative_walk( c, s, st, size, kSplitAt );
+            if ( end == kWalkSplit )
             {
-                const uint32_t take = min( size, 32u );
-                uint32_t       node = kNone;
-                if ( lane < take )
-                    node = st[ size - take + lane ];
-                size -= take;
-                __syncwarp();
-                bool     hit = false, eL = false, eR = false;
-                uint32_t lc = 0, rc = 0;
-                if ( node != kNone )
+                // hand the pending subtrees to other warps
+                uint32_t base = 0;
+                if ( lane == 0 )
+                    base = atomicAdd( b.sub_count, size );
+                base = __shfl_sync( 0xffffffffu, base, 0 );
+                if ( base + size <= b.sub_cap )
                 {
-                    if ( node >= n - 1 )
-                        hit = node < 2 * n - 1 && contributes( c, s, node - ( n - 1 ) );
-                    else
-                    {
-                        Box lb, rb;
-                        load_node( c.nodes, node, lb, rb, lc, rc );
-                        eL = enter_child( s, lb, lb.distance( s.bsph ) );
-                        eR = enter_child( s, rb, rb.distance( s.bsph ) );
-                    }
+                    for ( uint32_t q = lane; q < size; q += 32 )
+                        b.sub[ base + q ] = make_uint2( item, st[ q ] );
                 }
-                found = __any_sync( 0xffffffffu, hit );
-                uint32_t       total;
-                const uint32_t pushes = uint32_t( eL ) + uint32_t( eR );
-                uint32_t       off    = 0;
-                {
-                    uint32_t x = pushes;
-#pragma unroll
-                    for ( int o = 1; o < 32; o <<= 1 )
-                    {
-                        const uint32_t y = __shfl_up_sync( 0xffffffffu, x, o );
-                        if ( lane >= uint32_t( o ) )
-                            x += y;
-                    }
-                    total = __shfl_sync( 0xffffffffu, x, 31 );
-                    off   = x - pushes;
-                }
-                if ( size + total > kHeavyStack )
-                {
-                    overflow = true;
-                    break;
-                }
-                if ( eL )
-                    st[ size + off++ ] = lc;
-                if ( eR )
-                    st[ size + off ] = rc;
-                size += total;
-                __syncwarp();
+                else if ( lane == 0 )
+                    send_to_exact( b, s.t, s.e );
             }
-            if ( ( found || overflow ) && lane == 0 )
+            else if ( ( end == kWalkFound || end == kWalkOverflow ) && lane == 0 )
+                send_to_exact( b, s.t, s.e );
+            __syncwarp();
+        }
+    }
+
+    __global__ void __launch_bounds__( kHeavyBlock, 4 ) k_edge_heavy_sub( CellContext c, const uint32_t * __restrict__ tasks,
+                                                                          SpecBuffers b, uint32_t * error )
+    {
+        __shared__ uint32_t stacks[ kHeavyBlock / 32 ][ kHeavyStack ];
+        const uint32_t      warp  = threadIdx.x >> 5, lane = lane_of();
+        uint32_t *          st    = stacks[ warp ];
+        const uint32_t      count = min( *b.sub_count, b.sub_cap );
+        while ( true )
+        {
+            uint32_t q = 0;
+            if ( lane == 0 )
+                q = atomicAdd( b.sub_next, 1u );
+            q = __shfl_sync( 0xffffffffu, q, 0 );
+            if ( q >= count )
+                break;
+            const uint2 sub = b.sub[ q ];
+            const uint2 h   = b.heavy[ sub.x ];
+            if ( b.cell_flag[ h.x ] )
             {
-                // the exact path decides, searching this edge again
-                atomicOr( &b.maybe_bits[ size_t( s.t ) * kMaybeWords + ( s.e >> 5 ) ], 1u << ( s.e & 31 ) );
-                atomicOr( &b.cell_flag[ s.t ], kFlagFound );
+                if ( lane == 0 )
+                    atomicOr( &b.maybe_bits[ size_t( h.x ) * kMaybeWords + ( h.y >> 5 ) ], 1u << ( h.y & 31 ) );
+                continue;
             }
+            EdgeSearch s;
+            search_of_heavy( c, tasks, b, h, s );
+            uint32_t size = 1;
+            if ( lane == 0 )
+                st[ 0 ] = sub.y;
+            __syncwarp();
+            const uint32_t end = cooperative_walk( c, s, st, size, kHeavyStack + 1 );
+            if ( ( end == kWalkFound || end == kWalkOverflow ) && lane == 0 )
+                send_to_exact( b, s.t, s.e );
             __syncwarp();
         }
     }
@@ -540,13 +613,14 @@ namespace apo2
     }
 
     static size_t heavy_capacity( uint32_t n ) { return size_t( n ) + 1024; }
+    static size_t sub_capacity( uint32_t n ) { return 4 * size_t( n ) + 65536; }
 
     size_t spec_bytes( uint32_t n )
     {
         auto a = []( size_t x ) { return ( x + 255 ) & ~size_t( 255 ); };
         return a( 4 * size_t( n ) * kNbrCap ) + a( 4 * size_t( n ) ) * 4 + a( 4 * size_t( n ) ) + a( 16 ) * 3
                + a( 4 * output_scan_scratch_words( n ) ) + a( sizeof( uint2 ) * heavy_capacity( n ) ) + a( 16 ) * 2
-               + a( 4 * size_t( n ) * kMaybeWords );
+               + a( 4 * size_t( n ) * kMaybeWords ) + a( sizeof( uint2 ) * sub_capacity( n ) ) + a( 16 ) * 2;
     }
 
     void spec_carve( SpecBuffers & b, void * base, uint32_t n )
@@ -581,7 +655,14 @@ namespace apo2
         b.heavy_next = reinterpret_cast<uint32_t *>( p );
         p += a( 16 );
         b.maybe_bits = reinterpret_cast<uint32_t *>( p );
-        b.heavy_cap  = uint32_t( heavy_capacity( n ) );
+        p += a( 4 * size_t( n ) * kMaybeWords );
+        b.sub = reinterpret_cast<uint2 *>( p );
+        p += a( sizeof( uint2 ) * sub_capacity( n ) );
+        b.sub_count = reinterpret_cast<uint32_t *>( p );
+        p += a( 16 );
+        b.sub_next  = reinterpret_cast<uint32_t *>( p );
+        b.sub_cap   = uint32_t( sub_capacity( n ) );
+        b.heavy_cap = uint32_t( heavy_capacity( n ) );
     }
 
     static int g_spec_grid = 0, g_heavy_grid = 0;
@@ -606,8 +687,11 @@ namespace apo2
         cudaMemsetAsync( b.exact_count, 0, sizeof( uint32_t ), s );
         cudaMemsetAsync( b.heavy_count, 0, sizeof( uint32_t ), s );
         cudaMemsetAsync( b.heavy_next, 0, sizeof( uint32_t ), s );
+        cudaMemsetAsync( b.sub_count, 0, sizeof( uint32_t ), s );
+        cudaMemsetAsync( b.sub_next, 0, sizeof( uint32_t ), s );
         APO2_LAUNCH( "k_edge_speculate", s, k_edge_speculate<<<g_spec_grid, kSpecBlock, 0, s>>>( c, tasks, task_count, b, c.error ) );
         APO2_LAUNCH( "k_edge_heavy", s, k_edge_heavy<<<g_heavy_grid, kHeavyBlock, 0, s>>>( c, tasks, b, c.error ) );
+        APO2_LAUNCH( "k_edge_heavy_sub", s, k_edge_heavy_sub<<<g_heavy_grid, kHeavyBlock, 0, s>>>( c, tasks, b, c.error ) );
         APO2_LAUNCH( "k_edge_commit", s, k_edge_commit<<<std::max( 1u, std::min<uint32_t>( ( c.n + 7 ) / 8, 148 * 16 ) ), 256, 0, s>>>( c, tasks, task_count, b ) );
         SearchProof proof;
         proof.slots      = b.exact_slot;
