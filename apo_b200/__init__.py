@@ -29,6 +29,7 @@ APO2_OK, APO2_ERR_INVALID_ARG, APO2_ERR_CAPACITY, APO2_ERR_ITER_LIMIT, APO2_ERR_
 APO2_ERR_NOT_BUILT, APO2_ERR_OUT_OF_MEMORY, APO2_ERR_TOO_LARGE = 5, 6, 7
 APO2_F32, APO2_F64 = 0, 1
 APO2_HOST, APO2_DEVICE = 0, 1
+APO2_NO_KNN_STEPS = 0xFFFFFFFF
 
 _STATUS_NAMES = {
     0: "APO2_OK", 1: "APO2_ERR_INVALID_ARG", 2: "APO2_ERR_CAPACITY", 3: "APO2_ERR_ITER_LIMIT",
@@ -45,7 +46,7 @@ class Apo2Error(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("k", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32),
                 ("device", ctypes.c_uint32), ("stage_timing", ctypes.c_uint32), ("edge_search", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 10)]
+                ("knn_steps", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 9)]
 
 
 class Stats(ctypes.Structure):
@@ -157,8 +158,8 @@ class Topology:
 class AlgorithmGPU:
     """Counterpart of `apo::gpu::AlgorithmGPU<K>` (algorithm.cuh:12-46)."""
 
-    def __init__(self, sites, k: int = 16, max_iterations: int = 10, device: int = 0, stage_timing: bool = False,
-                 edge_search: int = 0):
+    def __init__(self, sites, knnValidationStep: int = 1, k: int = 16, max_iterations: int = 10, device: int = 0,
+                 stage_timing: bool = False, edge_search: int = 0):
         lib = load_library()
         self._sites, dtype = _as_sites(sites)
         self.n = int(self._sites.shape[0])
@@ -169,6 +170,8 @@ class AlgorithmGPU:
         opt.device = device
         opt.stage_timing = 1 if stage_timing else 0
         opt.edge_search = edge_search
+        opt.knn_steps = APO2_NO_KNN_STEPS if knnValidationStep == 0 else knnValidationStep
+        self.knnValidationStep = knnValidationStep
         handle = ctypes.c_void_p()
         _check(lib.apo2_create(self._sites.ctypes.data, self.n, dtype, APO2_HOST, ctypes.byref(opt), ctypes.byref(handle)))
         self._h = handle

@@ -203,9 +203,23 @@ namespace
         record( h, 1, s );
         launch_tree( h->tree, n, h->input_d4, h->scene, h->sort, s );
         record( h, 2, s ); // bounds+Morton+sort+tree recorded as one span plus the sort below
-        launch_knn( h->cells, s );
-        record( h, 3, s );
-        launch_cells( h->cells, s );
+        // kNN steps (algorithm.inl:1535-1549); with several, the kNN span is the first
+        // step's search and the cells span everything after it
+        const uint32_t steps = h->options.knn_steps;
+        if ( steps == 0 )
+        {
+            // no kNN list is ever searched; the reference leaves them all empty (0xff bytes)
+            cudaMemsetAsync( h->cells.knn, 0xff, sizeof( uint32_t ) * size_t( n ) * h->cells.k, s );
+            record( h, 3, s );
+            launch_cells( h->cells, kCellsInitOnly, s );
+        }
+        for ( uint32_t step = 0; step < steps; step++ )
+        {
+            launch_knn( h->cells, step, s );
+            if ( step == 0 )
+                record( h, 3, s );
+            launch_cells( h->cells, step == 0 ? kCellsFirst : kCellsNext, s );
+        }
         record( h, 4, s );
         const uint32_t rounds = h->options.max_iterations;
         for ( uint32_t r = 0; r < rounds; r++ )
@@ -320,6 +334,12 @@ apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_
         opt.max_iterations = 10;
     if ( opt.edge_search > 1 )
         return fail( APO2_ERR_INVALID_ARG, "edge_search is 0 or 1" );
+    if ( opt.knn_steps == 0 )
+        opt.knn_steps = 1;
+    else if ( opt.knn_steps == APO2_NO_KNN_STEPS )
+        opt.knn_steps = 0;
+    else if ( opt.knn_steps > 64 )
+        return fail( APO2_ERR_INVALID_ARG, "knn_steps is at most 64" );
     opt.max_iterations = std::min( opt.max_iterations, 64u );
 
     APO2_CUDA( cudaSetDevice( int( opt.device ) ), "cudaSetDevice" );

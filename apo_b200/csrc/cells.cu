@@ -631,7 +631,10 @@ namespace apo2
         }
     }
 
-    __global__ void __launch_bounds__( kKnnBlock ) k_knn( CellContext c )
+    // kNN step `step` (algorithm.inl:32-99): step 0 takes the k nearest sites and flags buried
+    // sites; a later step takes the next k, beyond the last neighbour of the previous step, or
+    // none once the previous list ran short.
+    __global__ void __launch_bounds__( kKnnBlock ) k_knn( CellContext c, uint32_t step )
     {
         __shared__ uint32_t s_keys[ kMaxK * kKnnBlock ];
         __shared__ float    s_dist[ kMaxK * kKnnBlock ];
@@ -639,6 +642,20 @@ namespace apo2
         if ( id >= c.n )
             return;
         const uint32_t k      = c.k;
+        const uint32_t n      = c.n;
+        const float4   si     = c.sites_f[ id ];
+        float          start  = -FLT_MAX;
+        if ( step != 0 )
+        {
+            const uint32_t last = c.knn[ size_t( id ) * k + k - 1 ];
+            if ( last >= n )
+            {
+                for ( uint32_t q = 0; q < k; q++ )
+                    c.knn[ size_t( id ) * k + q ] = kNone;
+                return;
+            }
+            start = sphere_distance( c.sites_f[ last ], si );
+        }
         uint32_t *     keys   = s_keys + threadIdx.x;
         float *        dist   = s_dist + threadIdx.x;
         const uint32_t stride = kKnnBlock;
@@ -647,15 +664,13 @@ namespace apo2
             keys[ q * stride ] = kNone;
             dist[ q * stride ] = FLT_MAX;
         }
-        const float4   si   = c.sites_f[ id ];
-        const uint32_t n    = c.n;
         uint32_t       err  = 0;
-        c.known_radii[ id ] = -FLT_MAX;
+        if ( step == 0 )
+            c.known_radii[ id ] = -FLT_MAX;
         uint8_t buried      = kInValidation;
         uint2          stack[ kStack ];
         int            sp   = 0;
         uint32_t       node = 0;
-        const float    start = -FLT_MAX;
         uint32_t       steps = 0;
         while ( true )
         {
@@ -730,6 +745,8 @@ namespace apo2
             c.knn[ size_t( id ) * k + q ] = keys[ q * stride ];
         if ( err )
             atomicOr( c.error, err );
+        if ( step != 0 )
+            return;
 
         // buried site: inside its nearest neighbour (algorithm.inl:85-98); `si` is the float copy
         const uint32_t nearest = keys[ 0 ];
@@ -769,7 +786,12 @@ namespace apo2
         __syncwarp();
     }
 
-    __global__ void __launch_bounds__( kCellBlock, 4 ) k_cells( CellContext c )
+    // Cell construction from the kNN lists (getCells, algorithm.inl:101-206). kCellsFirst
+    // starts every cell from the initial cell of the six bounding sites (the reference's
+    // initializeDataStructure, topology_update.inl:5-47, fused in); kCellsNext continues the
+    // stored cells with the next kNN step; kCellsInitOnly writes the initial cells, statuses
+    // and known radii alone (no kNN step at all).
+    __global__ void __launch_bounds__( kCellBlock, 4 ) k_cells( CellContext c, uint32_t mode )
     {
         extern __shared__ __align__( 16 ) unsigned char smem[];
         const uint32_t warp  = threadIdx.x >> 5;
@@ -779,11 +801,26 @@ namespace apo2
         uint32_t       err   = 0;
         for ( uint32_t i = gwarp; i < c.n; i += nwarp )
         {
+            if ( mode == kCellsInitOnly )
+            {
+                initial_cell( c, w, c.sites[ i ] );
+                store_cell( c, w, i, 0, err );
+                if ( lane_id() == 0 )
+                {
+                    c.status[ i ]      = kInValidation;
+                    c.known_radii[ i ] = -FLT_MAX;
+                }
+                __syncwarp();
+                continue;
+            }
             const uint8_t status = c.status[ i ];
-            if ( status == kFullyValidated )
+            if ( status == kFullyValidated || ( mode == kCellsNext && status == kBuried ) )
                 continue;
             const double4 si = c.sites[ i ];
-            initial_cell( c, w, si );
+            if ( mode == kCellsNext )
+                load_cell( c, w, i, si, true, true );
+            else
+                initial_cell( c, w, si );
             if ( status == kBuried )
             {
                 // a buried cell keeps the initial store (topology_update.inl:5-47)
@@ -1777,14 +1814,14 @@ namespace apo2
         return std::max( 1, std::min( g_cell_grid, needed ) );
     }
 
-    void launch_knn( const CellContext & c, cudaStream_t s )
+    void launch_knn( const CellContext & c, uint32_t step, cudaStream_t s )
     {
-        APO2_LAUNCH( "k_knn", s, k_knn<<<( c.n + kKnnBlock - 1 ) / kKnnBlock, kKnnBlock, 0, s>>>( c ) );
+        APO2_LAUNCH( "k_knn", s, k_knn<<<( c.n + kKnnBlock - 1 ) / kKnnBlock, kKnnBlock, 0, s>>>( c, step ) );
     }
 
-    void launch_cells( const CellContext & c, cudaStream_t s )
+    void launch_cells( const CellContext & c, uint32_t mode, cudaStream_t s )
     {
-        APO2_LAUNCH( "k_cells", s, k_cells<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c ) );
+        APO2_LAUNCH( "k_cells", s, k_cells<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, mode ) );
     }
 
     void launch_tasks( const CellContext & c, uint32_t * tasks, uint32_t * count, cudaStream_t s )

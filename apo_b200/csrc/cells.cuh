@@ -84,8 +84,12 @@ namespace apo2
         return float( r ) * 1.0001f + 1e-3f;
     }
     void configure_cell_kernels();
-    void launch_knn( const CellContext & c, cudaStream_t s );
-    void launch_cells( const CellContext & c, cudaStream_t s );
+    // k_cells modes: first kNN step, a later kNN step, initial cells only (no kNN step)
+    constexpr uint32_t kCellsFirst    = 0;
+    constexpr uint32_t kCellsNext     = 1;
+    constexpr uint32_t kCellsInitOnly = 2;
+    void launch_knn( const CellContext & c, uint32_t step, cudaStream_t s );
+    void launch_cells( const CellContext & c, uint32_t mode, cudaStream_t s );
     void launch_tasks( const CellContext & c, uint32_t * tasks, uint32_t * count, cudaStream_t s );
     void launch_vertex_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s );
     constexpr uint32_t kMaybeWords = ( kMaxEdges + 31 ) / 32; // 9 words of edge bits per task

@@ -37,6 +37,36 @@ UNIT = "sites/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
+# FP64 operation counts of the two innermost routines as written (add, mul, div and sqrt count
+# one each; comparisons none): the quadrisector solve with both roots (apo_b200/csrc/geometry.cuh,
+# after gpu/math.cuh:703-780) and the sphere-distance conflict test (gpu/math.cuh:368-388).
+C_QUAD = 216
+C_TEST = 11
+
+# DRAM bytes (read + write) per site of one build, by kernel, from one ncu capture of the
+# protein-like packing at 100,000 sites (profiles/top_kernels_protein100k.md), scaled by the
+# sites processed.
+TRAFFIC_BYTES_PER_SITE = {"k_vertex_validation": 1871.8, "k_edge_speculate": 1527.0, "k_cells": 304.0}
+
+
+def measure_fp64_peak(device) -> float:
+    """Dense FP64 throughput of this GPU in TFLOP/s: cuBLAS DGEMM 4096^3, best of 5."""
+    import torch
+    a = torch.randn(4096, 4096, dtype=torch.float64, device=device)
+    b = torch.randn(4096, 4096, dtype=torch.float64, device=device)
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * 4096 ** 3 / (best / 1e3) / 1e12
+
+
 def load_peaks() -> tuple[dict, str]:
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -246,17 +276,29 @@ def run_ours(args, world, rank, local):
     # share of the build's kernel time
     q = vcount
     b_alg = 16 * n + 32 * q + 8 * n
+    # algorithmic FP64 work (per diagram): every vertex is solved by its 4 cells and tested
+    # against K neighbours -- 4 Q (C_QUAD + K C_TEST)
+    f_alg = 4 * q * (C_QUAD + 16 * C_TEST)
+    fp64_peak = measure_fp64_peak(device)
     dom_bytes_per_launch = b_alg * (dom_ms / total_ms) / max(1, dom_count)
     dom_avg_ms = dom_ms / max(1, dom_count)
     achieved = dom_bytes_per_launch / (dom_avg_ms / 1e3) / 1e9
     roofline = {
         "bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-        "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_kind": peaks_kind,
+        "frac": achieved / peaks["hbm_gbs"],
+        "traffic": (TRAFFIC_BYTES_PER_SITE[dom_name] * n / max(1, dom_count)
+                    if dom_name in TRAFFIC_BYTES_PER_SITE else None),
+        "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, from a 100k-site capture "
+                        "scaled by sites", "peak_kind": peaks_kind,
         "kernel_share": dom_ms / total_ms, "kernel_avg_launch_ms": dom_avg_ms, "kernel_launches": dom_count,
         "algorithmic_bytes_per_diagram": b_alg,
         "note": "path is FP64- and latency-bound (BVH walks, warp-collective cell updates), not HBM-bound; "
                 "see profiles/ for FP64 pipe and DRAM counters",
         "build_algorithmic_gbs": b_alg / (ms_max / 1e3) / 1e9,
+        "fp64": {"achieved": f_alg / (ms_max / 1e3) / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+                 "frac": f_alg / (ms_max / 1e3) / 1e12 / fp64_peak if fp64_peak else None,
+                 "algorithmic_flop_per_diagram": f_alg, "c_quad": C_QUAD, "c_test": C_TEST,
+                 "peak_kind": "measured here: cuBLAS DGEMM 4096^3 through torch, best of 5"},
     }
 
     # --- end to end through the public API with host buffers ---
@@ -322,7 +364,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="protein1m")
     ap.add_argument("--sites", type=int, default=None)
-    ap.add_argument("--cpu-sample", type=int, default=20000)
+    ap.add_argument("--cpu-sample", type=int, default=100000)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()

@@ -116,6 +116,7 @@ namespace apo
                 options.struct_size  = sizeof( apo2_options );
                 options.k            = K;
                 options.stage_timing = 1;
+                options.knn_steps    = knnValidationStep == 0 ? APO2_NO_KNN_STEPS : knnValidationStep;
                 check( apo2_create( sites.ptr, m_siteNb, sizeof( Real ) == 8 ? APO2_F64 : APO2_F32, APO2_HOST, &options,
                                     &m_handle ) );
             }

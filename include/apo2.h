@@ -70,8 +70,13 @@ typedef struct apo2_options
     uint32_t stage_timing;         /* 1 = record per-stage CUDA-event times (apo2_stats) */
     uint32_t edge_search;          /* 0 = edge-parallel search with exact per-cell fallback (default),
                                       1 = warp-per-cell edge validation only; both give the same result */
-    uint32_t reserved[ 10 ];
+    uint32_t knn_steps;            /* kNN + cell-construction steps, the reference's knnValidationStep
+                                      (algorithm.inl:1535-1549): 0 = 1 (its default), APO2_NO_KNN_STEPS
+                                      = none (every cell starts from the initial cell), at most 64 */
+    uint32_t reserved[ 9 ];
 } apo2_options;
+
+#define APO2_NO_KNN_STEPS 0xffffffffu
 
 /* Per-build statistics, the counterpart of AlgorithmGPU::Sample (algorithm.cuh:18-27). */
 typedef struct apo2_stats

@@ -422,7 +422,9 @@ namespace
 #pragma omp atomic
             counters[ c ] += v;
         }
-        uint32_t             n = 0;
+        uint32_t             n        = 0;
+        uint32_t             k        = kK; // neighbours per kNN step (the AlgorithmGPU<K> argument)
+        uint32_t             knnSteps = 1;  // knnValidationStep (algorithm.inl:1535)
         std::vector<D4>      sites; // n + 6, Morton order then the 6 artificial sites
         std::vector<uint8_t> status;
         // LBVH (lbvh.cuh:9-62)
@@ -681,18 +683,33 @@ namespace
         }
     }
 
-    void knnSite( Context & ctx, uint32_t id )
+    // getKnns<K> (algorithm.inl:32-99): step 0 takes the K nearest and flags buried sites;
+    // a later step the next K beyond the previous step's last neighbour, or none once the
+    // previous list ran short.
+    void knnSite( Context & ctx, uint32_t id, uint32_t step )
     {
-        const uint32_t n = ctx.n;
+        const uint32_t n  = ctx.n;
+        const uint32_t kk = ctx.k;
         const F4       si = toFloat( ctx.sites[ id ] );
-        uint32_t       keys[ kK ];
-        float          dist[ kK ];
-        for ( uint32_t k = 0; k < kK; k++ )
+        float          startingDistance = -FLT_MAX;
+        if ( step != 0 )
+        {
+            const uint32_t last = ctx.knn[ std::size_t( id ) * kk + kk - 1 ];
+            if ( last >= n )
+            {
+                for ( uint32_t k = 0; k < kk; k++ )
+                    ctx.knn[ std::size_t( id ) * kk + k ] = kNone;
+                return;
+            }
+            startingDistance = sphereDistance( toFloat( ctx.sites[ last ] ), si );
+        }
+        uint32_t keys[ kK ];
+        float    dist[ kK ];
+        for ( uint32_t k = 0; k < kk; k++ )
         {
             keys[ k ] = kNone;
             dist[ k ] = FLT_MAX;
         }
-        const float startingDistance = -FLT_MAX;
 
         struct Entry { uint32_t node; float d; };
         Entry    stack[ 64 ];
@@ -734,7 +751,7 @@ namespace
                 {
                     dist[ 0 ] = d;
                     keys[ 0 ] = j;
-                    heapify( keys, dist, 0, kK );
+                    heapify( keys, dist, 0, kk );
                 }
             }
             bool more = false;
@@ -750,9 +767,11 @@ namespace
             if ( !more )
                 break;
         }
-        heapsort( keys, dist, int( kK ) );
-        for ( uint32_t k = 0; k < kK; k++ )
-            ctx.knn[ std::size_t( id ) * kK + k ] = keys[ k ];
+        heapsort( keys, dist, int( kk ) );
+        for ( uint32_t k = 0; k < kk; k++ )
+            ctx.knn[ std::size_t( id ) * kk + k ] = keys[ k ];
+        if ( step != 0 )
+            return;
 
         // buried test (algorithm.inl:85-98); `si` is the float copy of the site.
         if ( keys[ 0 ] == kNone )
@@ -1152,9 +1171,9 @@ namespace
             return;
         CellWork w { ctx, i, ctx.sites[ i ], ctx.cells[ i ], ctx.flags[ i ] };
         double   knownRadius = -DBL_MAX;
-        for ( uint32_t nId = 0; nId < kK; nId++ )
+        for ( uint32_t nId = 0; nId < ctx.k; nId++ )
         {
-            const uint32_t j = ctx.knn[ std::size_t( i ) * kK + nId ];
+            const uint32_t j = ctx.knn[ std::size_t( i ) * ctx.k + nId ];
             if ( j == kNone )
                 break;
             if ( ctx.status[ j ] == kBuried )
@@ -1819,8 +1838,9 @@ namespace
         if ( lastStage < ORACLE_STAGE_KNN )
             return;
 
-        ctx.knn.assign( std::size_t( n ) * kK, kNone );
-        parallelFor( n, threads, [ & ]( uint32_t id ) { knnSite( ctx, id ); } );
+        ctx.knn.assign( std::size_t( n ) * ctx.k, kNone );
+        if ( ctx.knnSteps > 0 )
+            parallelFor( n, threads, [ & ]( uint32_t id ) { knnSite( ctx, id, 0 ); } );
         if ( lastStage < ORACLE_STAGE_CELLS )
             return;
 
@@ -1828,7 +1848,12 @@ namespace
         ctx.knownRadii.assign( n, -FLT_MAX );
         for ( uint32_t i = 0; i < n; i++ )
             initialCell( ctx, ctx.cells[ i ] );
-        parallelFor( n, threads, [ & ]( uint32_t i ) { cellFromKnn( ctx, i ); } );
+        for ( uint32_t step = 0; step < ctx.knnSteps; step++ )
+        {
+            if ( step > 0 )
+                parallelFor( n, threads, [ & ]( uint32_t id ) { knnSite( ctx, id, step ); } );
+            parallelFor( n, threads, [ & ]( uint32_t i ) { cellFromKnn( ctx, i ); } );
+        }
 
         if ( lastStage >= ORACLE_STAGE_VALIDATION )
         {
@@ -1960,9 +1985,10 @@ struct oracle_run
 
 namespace
 {
-    oracle_run * buildFrom( std::vector<D4> && input, uint32_t n, int lastStage, int threads )
+    oracle_run * buildFrom( std::vector<D4> && input, uint32_t n, int lastStage, int threads, uint32_t k = kK,
+                            uint32_t knnSteps = 1 )
     {
-        if ( n < 2 )
+        if ( n < 2 || k < 1 || k > kK )
             return nullptr;
 #ifdef _OPENMP
         if ( threads <= 0 )
@@ -1971,7 +1997,9 @@ namespace
         threads = 1;
 #endif
         oracle_run * r = new oracle_run {};
-        r->ctx.n       = n;
+        r->ctx.n        = n;
+        r->ctx.k        = k;
+        r->ctx.knnSteps = knnSteps;
         run( r->ctx, input, lastStage, threads );
         return r;
     }
@@ -1993,6 +2021,26 @@ oracle_run * oracle_build_f64( const double * sites, uint32_t n, int lastStage, 
     for ( uint32_t i = 0; i < n; i++ )
         input[ i ] = { sites[ 4 * i ], sites[ 4 * i + 1 ], sites[ 4 * i + 2 ], sites[ 4 * i + 3 ] };
     return buildFrom( std::move( input ), n, lastStage, threads );
+}
+
+oracle_run * oracle_build_ex( const void * sites, int is_f64, uint32_t n, uint32_t k, uint32_t knn_steps, int lastStage,
+                              int threads )
+{
+    std::vector<D4> input( n );
+    for ( uint32_t i = 0; i < n; i++ )
+    {
+        if ( is_f64 )
+        {
+            const double * p = static_cast<const double *>( sites ) + 4 * std::size_t( i );
+            input[ i ]       = { p[ 0 ], p[ 1 ], p[ 2 ], p[ 3 ] };
+        }
+        else
+        {
+            const float * p = static_cast<const float *>( sites ) + 4 * std::size_t( i );
+            input[ i ]      = { p[ 0 ], p[ 1 ], p[ 2 ], p[ 3 ] };
+        }
+    }
+    return buildFrom( std::move( input ), n, lastStage, threads, k, knn_steps );
 }
 
 uint64_t oracle_get( const oracle_run * r, const char * name, const void ** data )

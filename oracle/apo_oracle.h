@@ -47,6 +47,12 @@ oracle_run * oracle_build( const float * sites_xyzr, uint32_t n, int last_stage,
 /* Same input given as float64 (x, y, z, r), as the reference's FP64 public API takes it. */
 oracle_run * oracle_build_f64( const double * sites_xyzr, uint32_t n, int last_stage, int threads );
 
+/* General form: float32 (is_f64 = 0) or float64 input, `k` neighbours per kNN step (1..16,
+ * the AlgorithmGPU<K> argument) and `knn_steps` kNN + cell steps (the knnValidationStep
+ * argument, algorithm.inl:1535-1549; 0 = none). */
+oracle_run * oracle_build_ex( const void * sites_xyzr, int is_f64, uint32_t n, uint32_t k, uint32_t knn_steps,
+                              int last_stage, int threads );
+
 /* Looks up one result array by name; returns its element count (0 if absent) and its
  * address in *data. Names: indices parent left right aabb sizes morton sites_sorted
  * status knn known_radii vertex_nb edge_nb vertices edges out_vertices out_vertices_id

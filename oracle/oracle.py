@@ -51,6 +51,9 @@ def _load():
         lib.oracle_build.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]
         lib.oracle_build_f64.restype = ctypes.c_void_p
         lib.oracle_build_f64.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]
+        lib.oracle_build_ex.restype = ctypes.c_void_p
+        lib.oracle_build_ex.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_int, ctypes.c_int]
         lib.oracle_get.restype = ctypes.c_uint64
         lib.oracle_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]
         lib.oracle_flags.restype = ctypes.c_uint32
@@ -60,12 +63,18 @@ def _load():
     return _lib
 
 
-def build(sites: np.ndarray, stage: int = STAGE_OUTPUT, threads: int = 0) -> dict:
-    """Runs the oracle on float32 (n, 4) sites; returns every result array by name."""
+def build(sites: np.ndarray, stage: int = STAGE_OUTPUT, threads: int = 0, k: int = 16, knn_steps: int = 1) -> dict:
+    """Runs the oracle on float32 or float64 (n, 4) sites; returns every result array by name.
+    `k` and `knn_steps` are the reference's AlgorithmGPU<K> and knnValidationStep arguments."""
     lib = _load()
     sites = np.ascontiguousarray(sites)
     n = sites.shape[0]
-    if sites.dtype == np.float64:
+    if (k, knn_steps) != (16, 1):
+        is_f64 = sites.dtype == np.float64
+        if not is_f64:
+            sites = np.ascontiguousarray(sites, dtype=np.float32)
+        handle = lib.oracle_build_ex(sites.ctypes.data, int(is_f64), n, k, knn_steps, stage, threads)
+    elif sites.dtype == np.float64:
         handle = lib.oracle_build_f64(sites.ctypes.data, n, stage, threads)
     else:
         sites = np.ascontiguousarray(sites, dtype=np.float32)

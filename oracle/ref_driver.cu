@@ -1,6 +1,7 @@
 // Driver for the reference library built from its own sources (oracle/ref_build.sh).
 //
-// It runs the reference's public path -- `AlgorithmGPU<16>{sites}.build()` followed by
+// It runs the reference's public path -- `AlgorithmGPU<K>{sites, knnValidationStep}.build()`
+// (K = 16 and one kNN step unless --k / --knn-steps say otherwise) followed by
 // `toHostFull()` and `toTopology()` (apo/include/apo/gpu/algorithm.inl:1410-1821) -- on a
 // site file and writes every array the parity tests pin: the LBVH node arrays and the
 // Morton permutation (apo/src/gpu/lbvh.cu:274-323), the kNN lists of the first search
@@ -58,43 +59,10 @@ namespace
     }
 } // namespace
 
-int main( int argc, char ** argv )
+template<uint32_t K>
+void runReference( std::vector<apo::Real> & sites, const uint32_t n, const std::string & outDir, const int repeat,
+                   const bool dump, const uint32_t knnSteps, std::string & json )
 {
-    if ( argc < 3 )
-    {
-        std::fprintf( stderr, "usage: %s sites.f32 outdir [--time R] [--no-dump]\n", argv[ 0 ] );
-        return 1;
-    }
-    const std::string input  = argv[ 1 ];
-    const std::string outDir = argv[ 2 ];
-    int               repeat = 0;
-    bool              dump   = true;
-    for ( int a = 3; a < argc; a++ )
-    {
-        if ( !std::strcmp( argv[ a ], "--time" ) && a + 1 < argc )
-            repeat = std::atoi( argv[ ++a ] );
-        else if ( !std::strcmp( argv[ a ], "--no-dump" ) )
-            dump = false;
-    }
-
-    // Sites are stored as float32 (x, y, z, r); the reference's FP64 build reads `double`.
-    FILE * f = std::fopen( input.c_str(), "rb" );
-    if ( !f )
-    {
-        std::fprintf( stderr, "cannot open %s\n", input.c_str() );
-        return 2;
-    }
-    std::fseek( f, 0, SEEK_END );
-    const long bytes = std::ftell( f );
-    std::fseek( f, 0, SEEK_SET );
-    std::vector<float> raw( static_cast<std::size_t>( bytes ) / sizeof( float ) );
-    if ( std::fread( raw.data(), sizeof( float ), raw.size(), f ) != raw.size() )
-        return 2;
-    std::fclose( f );
-    std::vector<apo::Real> sites( raw.begin(), raw.end() );
-    const uint32_t         n = static_cast<uint32_t>( sites.size() / 4 );
-
-    std::string json = "{\"n\": " + std::to_string( n );
 
     if ( repeat > 0 )
     {
@@ -108,7 +76,7 @@ int main( int argc, char ** argv )
             cudaDeviceSynchronize();
             cudaEventRecord( start );
             {
-                apo::gpu::AlgorithmGPU<16> algorithm { apo::ConstSpan<apo::Real> { sites.data(), sites.size() } };
+                apo::gpu::AlgorithmGPU<K> algorithm { apo::ConstSpan<apo::Real> { sites.data(), sites.size() }, knnSteps };
                 algorithm.build();
                 if ( r >= 0 )
                 {
@@ -151,7 +119,7 @@ int main( int argc, char ** argv )
 
     if ( dump )
     {
-        apo::gpu::AlgorithmGPU<16> algorithm { apo::ConstSpan<apo::Real> { sites.data(), sites.size() } };
+        apo::gpu::AlgorithmGPU<K> algorithm { apo::ConstSpan<apo::Real> { sites.data(), sites.size() }, knnSteps };
         algorithm.build();
         check( "build" );
 
@@ -172,19 +140,19 @@ int main( int argc, char ** argv )
             writeArray( outDir, "sizes.u32", sizes.data(), sizes.size() );
         }
 
-        const auto sorted = download( algorithm.dSites.get<apo::Real>(), ( n + 6 ) * 4 );
+        const auto sorted = download( algorithm.dSites.template get<apo::Real>(), ( n + 6 ) * 4 );
         writeArray( outDir, "sites_sorted.f64", sorted.data(), sorted.size() );
 
-        const auto status = download( algorithm.dStatus.get<uint8_t>(), n );
+        const auto status = download( algorithm.dStatus.template get<uint8_t>(), n );
         writeArray( outDir, "status.u8", status.data(), status.size() );
 
-        const auto vertexNb = download( algorithm.dVerticesNb.get<uint32_t>(), n );
-        const auto edgeNb   = download( algorithm.dEdgesNb.get<uint32_t>(), n );
+        const auto vertexNb = download( algorithm.dVerticesNb.template get<uint32_t>(), n );
+        const auto edgeNb   = download( algorithm.dEdgesNb.template get<uint32_t>(), n );
         writeArray( outDir, "vertex_nb.u32", vertexNb.data(), vertexNb.size() );
         writeArray( outDir, "edge_nb.u32", edgeNb.data(), edgeNb.size() );
         {
-            const auto vertexStore = download( algorithm.dVertices.get<uint32_t>(), std::size_t( n ) * 152 * 4 );
-            const auto edgeStore   = download( algorithm.dEdges.get<uint32_t>(), std::size_t( n ) * 264 * 4 );
+            const auto vertexStore = download( algorithm.dVertices.template get<uint32_t>(), std::size_t( n ) * 152 * 4 );
+            const auto edgeStore   = download( algorithm.dEdges.template get<uint32_t>(), std::size_t( n ) * 264 * 4 );
             std::vector<uint32_t> vertices, edges;
             for ( uint32_t i = 0; i < n; i++ )
             {
@@ -206,15 +174,15 @@ int main( int argc, char ** argv )
         {
             apo::gpu::ContextCellOriented context {};
             context.siteNb   = n;
-            context.sites    = algorithm.dSites.get<apo::gpu::Real4>();
-            context.status   = algorithm.dStatus.get<uint8_t>();
+            context.sites    = algorithm.dSites.template get<apo::gpu::Real4>();
+            context.status   = algorithm.dStatus.template get<uint8_t>();
             uint32_t * knns  = nullptr;
-            cudaMalloc( &knns, sizeof( uint32_t ) * n * 16 );
-            cudaMemset( knns, 0xff, sizeof( uint32_t ) * n * 16 );
+            cudaMalloc( &knns, sizeof( uint32_t ) * n * K );
+            cudaMemset( knns, 0xff, sizeof( uint32_t ) * n * K );
             auto [ gridDim, blockDim ] = apo::gpu::KernelConfig::From( n, apo::gpu::impl::KnnBlockSize );
-            apo::gpu::impl::getKnns<16><<<gridDim, blockDim>>>( 0, context, view, knns );
+            apo::gpu::impl::getKnns<K><<<gridDim, blockDim>>>( 0, context, view, knns );
             check( "getKnns" );
-            const auto knnHost = download( knns, std::size_t( n ) * 16 );
+            const auto knnHost = download( knns, std::size_t( n ) * K );
             writeArray( outDir, "knn.u32", knnHost.data(), knnHost.size() );
             cudaFree( knns );
         }
@@ -233,6 +201,61 @@ int main( int argc, char ** argv )
 
         json += ", \"vertices\": " + std::to_string( full.vertices.size() / 4 );
         json += ", \"closed_edges\": " + std::to_string( full.closedEdgesMin.size() / 4 );
+    }
+
+}
+
+int main( int argc, char ** argv )
+{
+    if ( argc < 3 )
+    {
+        std::fprintf( stderr, "usage: %s sites.f32 outdir [--time R] [--no-dump] [--k 1|4|8|16] [--knn-steps S]\n", argv[ 0 ] );
+        return 1;
+    }
+    const std::string input  = argv[ 1 ];
+    const std::string outDir = argv[ 2 ];
+    int               repeat = 0;
+    bool              dump   = true;
+    uint32_t          k        = 16; // AlgorithmGPU<K>
+    uint32_t          knnSteps = 1;  // knnValidationStep
+    for ( int a = 3; a < argc; a++ )
+    {
+        if ( !std::strcmp( argv[ a ], "--time" ) && a + 1 < argc )
+            repeat = std::atoi( argv[ ++a ] );
+        else if ( !std::strcmp( argv[ a ], "--no-dump" ) )
+            dump = false;
+        else if ( !std::strcmp( argv[ a ], "--k" ) && a + 1 < argc )
+            k = uint32_t( std::atoi( argv[ ++a ] ) );
+        else if ( !std::strcmp( argv[ a ], "--knn-steps" ) && a + 1 < argc )
+            knnSteps = uint32_t( std::atoi( argv[ ++a ] ) );
+    }
+
+    // Sites are stored as float32 (x, y, z, r); the reference's FP64 build reads `double`.
+    FILE * f = std::fopen( input.c_str(), "rb" );
+    if ( !f )
+    {
+        std::fprintf( stderr, "cannot open %s\n", input.c_str() );
+        return 2;
+    }
+    std::fseek( f, 0, SEEK_END );
+    const long bytes = std::ftell( f );
+    std::fseek( f, 0, SEEK_SET );
+    std::vector<float> raw( static_cast<std::size_t>( bytes ) / sizeof( float ) );
+    if ( std::fread( raw.data(), sizeof( float ), raw.size(), f ) != raw.size() )
+        return 2;
+    std::fclose( f );
+    std::vector<apo::Real> sites( raw.begin(), raw.end() );
+    const uint32_t         n = static_cast<uint32_t>( sites.size() / 4 );
+
+    std::string json = "{\"n\": " + std::to_string( n );
+    json += ", \"k\": " + std::to_string( k ) + ", \"knn_steps\": " + std::to_string( knnSteps );
+    switch ( k )
+    {
+    case 1: runReference<1>( sites, n, outDir, repeat, dump, knnSteps, json ); break;
+    case 4: runReference<4>( sites, n, outDir, repeat, dump, knnSteps, json ); break;
+    case 8: runReference<8>( sites, n, outDir, repeat, dump, knnSteps, json ); break;
+    case 16: runReference<16>( sites, n, outDir, repeat, dump, knnSteps, json ); break;
+    default: std::fprintf( stderr, "k must be 1, 4, 8 or 16\n" ); return 1;
     }
 
     json += "}\n";

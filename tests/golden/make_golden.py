@@ -9,7 +9,13 @@ apo_b200.generators (named in CASES below), so only the outputs are stored.
 Small cases are stored whole (compressed .npz). For every case, each array's SHA-256 is
 recorded in digests.json, so larger cases are pinned without storing their arrays.
 
-Usage: python tests/golden/make_golden.py <dump_root>   (dump_root/<case>/*.u32 ...)
+Cases may set the AlgorithmGPU<K> template argument and the knnValidationStep constructor
+argument (default 16 and 1); the driver gets them as --k / --knn-steps.
+
+Usage:
+    python tests/golden/make_golden.py inputs <dir>   writes <case>.f32 and <case>.args per case
+    bash tests/golden/dump_reference.sh <dir> <dump_root>   (on a GPU: runs the reference driver)
+    python tests/golden/make_golden.py <dump_root>    (dump_root/<case>/*.u32 ...) -> fixtures
 """
 from __future__ import annotations
 
@@ -33,7 +39,18 @@ CASES = {
     "prec3": ("precision_cloud(3)", True),
     "uni2k": ("uniform_cloud(2000, 58.48, 1.5, 0.5)", True),
     "uniform_small": ("uniform_small()", False),
+    # several kNN steps, other K, and no kNN step at all (knnValidationStep = 0)
+    "uni2k_s2": ("uniform_cloud(2000, 58.48, 1.5, 0.5)", True, 16, 2),
+    "uni2k_k4s3": ("uniform_cloud(2000, 58.48, 1.5, 0.5)", True, 4, 3),
+    "prec1_k8s0": ("precision_cloud(1)", True, 8, 0),
+    "prec2_k1s4": ("precision_cloud(2)", True, 1, 4),
 }
+
+
+def case_params(case: str) -> tuple[int, int]:
+    """(K, knnValidationStep) of a case."""
+    entry = CASES[case]
+    return (entry[2], entry[3]) if len(entry) > 2 else (16, 1)
 
 ARRAYS = {
     "indices": np.uint32, "parent": np.int32, "left": np.int32, "right": np.int32,
@@ -66,17 +83,32 @@ def digest(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
+def write_inputs(out: str) -> None:
+    os.makedirs(out, exist_ok=True)
+    for case in CASES:
+        sites_for(case).astype(np.float32).tofile(os.path.join(out, case + ".f32"))
+        k, steps = case_params(case)
+        with open(os.path.join(out, case + ".args"), "w") as f:
+            f.write(f"--k {k} --knn-steps {steps}\n")
+
+
 def main(root: str) -> None:
-    digests = {}
-    for case, (_, whole) in CASES.items():
+    """Adds (or refreshes) the cases found under `root`; the other cases' digests stay."""
+    path = os.path.join(HERE, "digests.json")
+    digests = json.load(open(path)) if os.path.exists(path) else {}
+    for case, entry in CASES.items():
+        whole = entry[1]
         if not os.path.isdir(os.path.join(root, case)):
             print("skip", case)
             continue
         sites = sites_for(case)
         dump = load_dump(root, case)
         meta = json.load(open(os.path.join(root, case, "meta.json")))
+        k, steps = case_params(case)
         digests[case] = {
             "n": int(sites.shape[0]),
+            "k": k,
+            "knn_steps": steps,
             "sites_sha256": digest(sites),
             "vertices": int(meta.get("vertices", 0)),
             "closed_edges": int(meta.get("closed_edges", 0)),
@@ -86,9 +118,12 @@ def main(root: str) -> None:
         if whole:
             np.savez_compressed(os.path.join(HERE, f"{case}.npz"), **dump)
         print(case, sites.shape[0], "stored" if whole else "digests only")
-    with open(os.path.join(HERE, "digests.json"), "w") as f:
+    with open(path, "w") as f:
         json.dump(digests, f, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1])
+    if sys.argv[1] == "inputs":
+        write_inputs(sys.argv[2])
+    else:
+        main(sys.argv[1])

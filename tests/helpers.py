@@ -10,6 +10,10 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 # Cases stored whole under tests/golden (reference dumps), and those pinned by digest only.
 STORED_CASES = ["prec0", "prec1", "prec2", "prec3", "uni2k"]
+# Stored cases built with another K or number of kNN steps (the reference's AlgorithmGPU<K>
+# and knnValidationStep); their "knn" golden is the first step's list, so it is compared
+# only for single-step cases.
+STEP_CASES = ["uni2k_s2", "uni2k_k4s3", "prec1_k8s0", "prec2_k1s4"]
 DIGEST_CASES = ["uniform_small"]
 
 # Bit-exact arrays (integer / index work, and float arrays produced by exact operations).
@@ -36,6 +40,18 @@ def digests() -> dict:
 def sites_for(case: str) -> np.ndarray:
     from tests.golden.make_golden import sites_for as _s
     return _s(case)
+
+
+def case_params(case: str) -> tuple[int, int]:
+    """(K, knnValidationStep) the case was built with."""
+    from tests.golden.make_golden import case_params as _p
+    return _p(case)
+
+
+def exact_names(case: str) -> list[str]:
+    """The bit-exact arrays a case's golden pins."""
+    k, steps = case_params(case)
+    return [n for n in EXACT if n != "knn" or steps == 1]
 
 
 def sha(a: np.ndarray) -> str:

@@ -26,10 +26,11 @@ def apo():
     return apo_b200
 
 
-def _check_against_golden(apo, sites, golden, label):
-    algo = apo.AlgorithmGPU(sites)
+def _check_against_golden(apo, sites, golden, label, case=None):
+    k, steps = H.case_params(case) if case else (16, 1)
+    algo = apo.AlgorithmGPU(sites, knnValidationStep=steps, k=k)
     algo.build()
-    for name in H.EXACT:
+    for name in (H.exact_names(case) if case else H.EXACT):
         if name.startswith("topo_"):
             continue
         mine = algo.debug_array(name)
@@ -47,9 +48,25 @@ def _check_against_golden(apo, sites, golden, label):
     algo.close()
 
 
-@pytest.mark.parametrize("case", H.STORED_CASES)
+@pytest.mark.parametrize("case", H.STORED_CASES + H.STEP_CASES)
 def test_gpu_matches_reference_dump(apo, case):
-    _check_against_golden(apo, H.sites_for(case), H.load_golden(case), case)
+    _check_against_golden(apo, H.sites_for(case), H.load_golden(case), case, case)
+
+
+@pytest.mark.parametrize("k,steps", [(16, 3), (2, 5), (16, 0)])
+def test_gpu_knn_steps_match_oracle(apo, oracle_lib, k, steps):
+    """Several kNN steps, or none, on a 20k-site cloud: every store bit-identical to the oracle."""
+    from apo_b200 import generators as g
+    sites = g.uniform_random(20000, 127.0, 0.5, 2.0, 21)
+    ref = oracle_lib.build(sites, k=k, knn_steps=steps)
+    algo = apo.AlgorithmGPU(sites, knnValidationStep=steps, k=k)
+    algo.build()
+    for name in ["status", "knn", "vertex_nb", "edge_nb", "vertices", "edges"]:
+        assert np.array_equal(algo.debug_array(name), ref[name]), name
+    full = algo.toHostFull(True)
+    assert np.array_equal(full.verticesId, ref["out_vertices_id"])
+    assert H.rel_err(full.vertices, ref["out_vertices"]) <= H.ORACLE_POSITION_RTOL
+    algo.close()
 
 
 @pytest.mark.parametrize("case", H.STORED_CASES[:2])

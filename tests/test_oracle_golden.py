@@ -6,12 +6,13 @@ import pytest
 from tests import helpers as H
 
 
-@pytest.mark.parametrize("case", H.STORED_CASES)
+@pytest.mark.parametrize("case", H.STORED_CASES + H.STEP_CASES)
 def test_oracle_matches_reference_dump(case, oracle_lib):
     golden = H.load_golden(case)
-    r = oracle_lib.build(H.sites_for(case))
+    k, steps = H.case_params(case)
+    r = oracle_lib.build(H.sites_for(case), k=k, knn_steps=steps)
     assert r["flags"] == 0
-    for name in H.EXACT:
+    for name in H.exact_names(case):
         assert np.array_equal(r[name], golden[name]), f"{case}: {name} differs from the reference"
     assert np.array_equal(r["out_vertices_id"], golden["vertices_id"])
     assert np.array_equal(H.closed_ids3(r["out_closed_id"]), golden["closed_id"])
@@ -55,3 +56,30 @@ def test_oracle_threads_do_not_change_results(oracle_lib):
 def test_oracle_rejects_tiny_input(oracle_lib):
     with pytest.raises(ValueError):
         oracle_lib.build(np.zeros((1, 4), dtype=np.float32))
+
+
+def test_oracle_later_knn_steps_continue_the_lists(oracle_lib):
+    """A second kNN step takes the next K sites beyond the first step's last neighbour, so
+    two steps of K see the same neighbours as one step of 2K would (up to distance ties)."""
+    sites = H.sites_for("uni2k")
+    one = oracle_lib.build(sites, stage=2, k=8, knn_steps=1)
+    two = oracle_lib.build(sites, stage=3, k=8, knn_steps=2)
+    wide = oracle_lib.build(sites, stage=2, k=16, knn_steps=1)
+    first = one["knn"].reshape(-1, 8)
+    second = two["knn"].reshape(-1, 8)
+    both = np.concatenate([first, second], axis=1)
+    same = np.mean(np.all(np.sort(both, axis=1) == np.sort(wide["knn"].reshape(-1, 16), axis=1), axis=1))
+    assert same > 0.99
+    assert not np.intersect1d(first[0], second[0]).size
+
+
+def test_oracle_without_knn_steps_validates_every_cell(oracle_lib):
+    """knnValidationStep = 0: no kNN lists and no certificate, every cell is validated from
+    its initial cell, and no site is flagged buried."""
+    sites = H.sites_for("prec1")
+    r = oracle_lib.build(sites, stage=3, k=16, knn_steps=0)
+    assert np.all(r["knn"] == 0xFFFFFFFF)
+    assert np.all(r["status"] == 0)
+    assert np.all(r["vertex_nb"] == 8) and np.all(r["edge_nb"] == 12)
+    full = oracle_lib.build(sites, k=16, knn_steps=0)
+    assert full["flags"] == 0 and full["out_vertices_id"].size > 0
