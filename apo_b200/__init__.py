@@ -46,7 +46,7 @@ class Apo2Error(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("k", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32),
                 ("device", ctypes.c_uint32), ("stage_timing", ctypes.c_uint32), ("edge_search", ctypes.c_uint32),
-                ("knn_steps", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 9)]
+                ("knn_steps", ctypes.c_uint32), ("stop_after", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 8)]
 
 
 class Stats(ctypes.Structure):
@@ -159,7 +159,7 @@ class AlgorithmGPU:
     """Counterpart of `apo::gpu::AlgorithmGPU<K>` (algorithm.cuh:12-46)."""
 
     def __init__(self, sites, knnValidationStep: int = 1, k: int = 16, max_iterations: int = 10, device: int = 0,
-                 stage_timing: bool = False, edge_search: int = 0):
+                 stage_timing: bool = False, edge_search: int = 0, stop_after: int = 0):
         lib = load_library()
         self._sites, dtype = _as_sites(sites)
         self.n = int(self._sites.shape[0])
@@ -171,6 +171,7 @@ class AlgorithmGPU:
         opt.stage_timing = 1 if stage_timing else 0
         opt.edge_search = edge_search
         opt.knn_steps = APO2_NO_KNN_STEPS if knnValidationStep == 0 else knnValidationStep
+        opt.stop_after = stop_after
         self.knnValidationStep = knnValidationStep
         handle = ctypes.c_void_p()
         _check(lib.apo2_create(self._sites.ctypes.data, self.n, dtype, APO2_HOST, ctypes.byref(opt), ctypes.byref(handle)))

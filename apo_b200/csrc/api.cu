@@ -221,18 +221,26 @@ namespace
             launch_cells( h->cells, step == 0 ? kCellsFirst : kCellsNext, s );
         }
         record( h, 4, s );
+        // stop_after (parity checks): 1 after the cells, 2 + 2r / 3 + 2r after round r's passes
+        const uint32_t stop   = h->options.stop_after;
+        bool           halted = stop == 1;
         const uint32_t rounds = h->options.max_iterations;
-        for ( uint32_t r = 0; r < rounds; r++ )
+        cudaMemsetAsync( h->task_counts, 0, sizeof( uint32_t ) * rounds, s );
+        for ( uint32_t r = 0; r < rounds && !halted; r++ )
         {
             launch_tasks( h->cells, h->tasks, h->task_counts + r, s );
             launch_vertex_validation( h->cells, h->tasks, h->task_counts + r, s );
+            if ( stop == 2 + 2 * r )
+                break;
             if ( h->options.edge_search == 1 )
                 launch_edge_validation( h->cells, h->tasks, h->task_counts + r, s );
             else
                 launch_edge_validation_speculative( h->cells, h->tasks, h->task_counts + r, h->spec, s );
+            halted = stop == 3 + 2 * r;
         }
         record( h, 5, s );
-        launch_bisector_validation( h->cells, s );
+        if ( stop == 0 )
+            launch_bisector_validation( h->cells, s );
         record( h, 6, s );
         const cudaError_t err = cudaGetLastError();
         if ( err != cudaSuccess )

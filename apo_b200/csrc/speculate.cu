@@ -26,6 +26,14 @@ namespace apo2
     constexpr uint32_t kHeavyBlock    = 128;
     constexpr uint32_t kHeavyStack    = 3072; // shared node stack per warp of the cooperative walk
     constexpr uint32_t kSplitAt       = 192;  // pending subtrees at which a long walk is handed out
+#ifndef APO2_SPEC_REFILL_AT
+#define APO2_SPEC_REFILL_AT 24
+#endif
+    // Idle lanes of a speculation warp fetch and set up new edges together, once at least
+    // this many are idle (or none is walking): the set-up (bounding sphere, certificate test)
+    // is long FP64 code, and run by one or two lanes at a time it held the warp for most
+    // of its time.
+    constexpr uint32_t kRefillAt = APO2_SPEC_REFILL_AT;
 
     __device__ __forceinline__ uint32_t lane_of() { return threadIdx.x & 31; }
 
@@ -284,64 +292,82 @@ namespace apo2
         uint32_t       err   = 0;
 
         EdgeSearch s;
-        bool       active = false;
+        bool       active    = false;
+        bool       exhausted = false; // the queue is empty for this lane
         uint32_t   stack[ kStack ];
         int        sp    = 0;
         uint32_t   node  = 0;
         uint32_t   steps = 0;
         while ( true )
         {
-            if ( !active )
+            // warp-uniform choice between a refill round and a walk step
+            const uint32_t idle = __ballot_sync( 0xffffffffu, !active && !exhausted );
+            const uint32_t busy = __ballot_sync( 0xffffffffu, active );
+            if ( idle == 0 && busy == 0 )
+                break;
+            if ( idle != 0 && ( busy == 0 || uint32_t( __popc( idle ) ) >= kRefillAt ) )
             {
-                // warp-aggregated fetch of the next item
-                const uint32_t mask   = __activemask();
-                const uint32_t leader = __ffs( mask ) - 1;
-                uint64_t       base   = 0;
-                if ( lane_of() == leader )
-                    base = atomicAdd( reinterpret_cast<unsigned long long *>( b.item_counter ), __popc( mask ) );
-                base                 = __shfl_sync( mask, base, leader );
-                const uint64_t item  = base + __popc( mask & ( ( 1u << lane_of() ) - 1u ) );
-                if ( item >= total )
-                    break;
-                // task holding this item: last t with offset[t] <= item
-                uint32_t lo = 0, hi = count;
-                while ( hi - lo > 1 )
+                if ( !active && !exhausted )
                 {
-                    const uint32_t mid = ( lo + hi ) >> 1;
-                    if ( b.item_offset[ mid ] <= item )
-                        lo = mid;
+                    // warp-aggregated fetch of the next item by the idle lanes
+                    const uint32_t leader = __ffs( idle ) - 1;
+                    uint64_t       base   = 0;
+                    if ( lane_of() == leader )
+                        base = atomicAdd( reinterpret_cast<unsigned long long *>( b.item_counter ), __popc( idle ) );
+                    base                = __shfl_sync( idle, base, leader );
+                    const uint64_t item = base + __popc( idle & ( ( 1u << lane_of() ) - 1u ) );
+                    if ( item >= total )
+                        exhausted = true;
                     else
-                        hi = mid;
+                    {
+                        // task holding this item: last t with offset[t] <= item
+                        uint32_t lo = 0, hi = count;
+                        while ( hi - lo > 1 )
+                        {
+                            const uint32_t mid = ( lo + hi ) >> 1;
+                            if ( b.item_offset[ mid ] <= item )
+                                lo = mid;
+                            else
+                                hi = mid;
+                        }
+                        s.t              = lo;
+                        const uint32_t e = uint32_t( item - b.item_offset[ s.t ] );
+                        s.e              = e;
+                        if ( b.cell_flag[ s.t ] )
+                        {
+                            // the cell goes to the exact path anyway; leave this edge undecided there
+                            atomicOr( &b.maybe_bits[ size_t( s.t ) * kMaybeWords + ( e >> 5 ) ], 1u << ( e & 31 ) );
+                        }
+                        else
+                        {
+                            s.i           = tasks[ s.t ];
+                            const uint4 r = c.edges[ size_t( s.i ) * kMaxEdges + e ];
+                            s.k           = r.x;
+                            s.l           = r.y;
+                            s.closed      = r.z == kNone;
+                            s.si          = c.sites[ s.i ];
+                            s.nbr         = b.nbr + size_t( s.t ) * kNbrCap;
+                            s.nbr_count   = b.nbr_count[ s.t ];
+                            // an edge validated before is not searched (algorithm.inl:522-526, 552)
+                            if ( ( r.w & 0xffu ) != 1u )
+                            {
+                                s.sk = c.sites[ s.k ];
+                                s.sl = c.sites[ s.l ];
+                                if ( setup_edge( c, s, c.known_radii[ s.i ] ) )
+                                {
+                                    active = true;
+                                    sp     = 0;
+                                    node   = 0;
+                                    steps  = 0;
+                                }
+                            }
+                        }
+                    }
                 }
-                s.t = lo;
-                if ( b.cell_flag[ s.t ] )
-                {
-                    // the cell goes to the exact path anyway; leave this edge undecided there
-                    const uint32_t e0 = uint32_t( item - b.item_offset[ s.t ] );
-                    atomicOr( &b.maybe_bits[ size_t( s.t ) * kMaybeWords + ( e0 >> 5 ) ], 1u << ( e0 & 31 ) );
-                    continue;
-                }
-                s.i              = tasks[ s.t ];
-                const uint32_t e = uint32_t( item - b.item_offset[ s.t ] );
-                s.e              = e;
-                const uint4    r = c.edges[ size_t( s.i ) * kMaxEdges + e ];
-                s.k              = r.x;
-                s.l              = r.y;
-                s.closed         = r.z == kNone;
-                s.si             = c.sites[ s.i ];
-                s.nbr            = b.nbr + size_t( s.t ) * kNbrCap;
-                s.nbr_count      = b.nbr_count[ s.t ];
-                if ( ( r.w & 0xffu ) == 1u )
-                    continue; // validated before: not searched (algorithm.inl:522-526, 552)
-                s.sk = c.sites[ s.k ];
-                s.sl = c.sites[ s.l ];
-                if ( !setup_edge( c, s, c.known_radii[ s.i ] ) )
-                    continue;
-                active = true;
-                sp     = 0;
-                node   = 0;
-                steps  = 0;
+                continue;
             }
+            if ( !active )
+                continue;
 
             // one step of the walk: descend to a leaf (or prune), test it, pop
             if ( ++steps > kLaneBudget )

@@ -73,7 +73,10 @@ typedef struct apo2_options
     uint32_t knn_steps;            /* kNN + cell-construction steps, the reference's knnValidationStep
                                       (algorithm.inl:1535-1549): 0 = 1 (its default), APO2_NO_KNN_STEPS
                                       = none (every cell starts from the initial cell), at most 64 */
-    uint32_t reserved[ 9 ];
+    uint32_t stop_after;           /* parity checks only: 0 = the whole build; 1 = stop after the kNN
+                                      cell construction; 2 + 2r / 3 + 2r = stop after the vertex / edge
+                                      validation of round r (0-based). Output extraction still works */
+    uint32_t reserved[ 8 ];
 } apo2_options;
 
 #define APO2_NO_KNN_STEPS 0xffffffffu

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -58,6 +59,146 @@ namespace
         }
     }
 } // namespace
+
+
+// --stages: the reference's build sequence (algorithm.inl:1410-1594), stage by stage, calling
+// its own kernels, with the per-cell stores dumped after the kNN cells ("s1"), after each
+// round's vertex ("v<r>") and edge ("e<r>") validation, and after bisector validation ("b").
+// Used to find the first stage at which another implementation departs from the reference.
+namespace apo::gpu
+{
+    // `length` looked up from inside apo::gpu, as build() does
+    inline Real stagedLength( Real3 v ) { return length( v ); }
+} // namespace apo::gpu
+
+template<uint32_t K>
+struct StagedBuild : apo::gpu::AlgorithmGPU<K>
+{
+    using Base = apo::gpu::AlgorithmGPU<K>;
+    using Base::Base;
+
+    void dump( const std::string & dir, const std::string & tag, const float * knownRadii )
+    {
+        const uint32_t n        = this->m_siteNb;
+        check( tag.c_str() );
+        const auto vertexNb = download( this->dVerticesNb.template get<uint32_t>(), n );
+        const auto edgeNb   = download( this->dEdgesNb.template get<uint32_t>(), n );
+        const auto status   = download( this->dStatus.template get<uint8_t>(), n );
+        const auto radii    = download( knownRadii, n );
+        const auto vstore   = download( this->dVertices.template get<uint32_t>(), std::size_t( n ) * 152 * 4 );
+        const auto estore   = download( this->dEdges.template get<uint32_t>(), std::size_t( n ) * 264 * 4 );
+        std::vector<uint32_t> vertices, edges;
+        for ( uint32_t i = 0; i < n; i++ )
+        {
+            const uint32_t vn = std::min( vertexNb[ i ], 152u ), en = std::min( edgeNb[ i ], 264u );
+            vertices.insert( vertices.end(), vstore.begin() + std::size_t( i ) * 608, vstore.begin() + std::size_t( i ) * 608 + vn * 4 );
+            edges.insert( edges.end(), estore.begin() + std::size_t( i ) * 1056, estore.begin() + std::size_t( i ) * 1056 + en * 4 );
+        }
+        writeArray( dir, ( tag + "_vertex_nb.u32" ).c_str(), vertexNb.data(), vertexNb.size() );
+        writeArray( dir, ( tag + "_edge_nb.u32" ).c_str(), edgeNb.data(), edgeNb.size() );
+        writeArray( dir, ( tag + "_status.u8" ).c_str(), status.data(), status.size() );
+        writeArray( dir, ( tag + "_known_radii.f32" ).c_str(), radii.data(), radii.size() );
+        writeArray( dir, ( tag + "_vertices.u32" ).c_str(), vertices.data(), vertices.size() );
+        writeArray( dir, ( tag + "_edges.u32" ).c_str(), edges.data(), edges.size() );
+    }
+
+    void stagedBuild( const std::string & dir )
+    {
+        using namespace apo::gpu;
+        using apo::Real;
+        const uint32_t n = this->m_siteNb;
+
+        ContextCellOriented context {};
+        context.siteNb    = n;
+        this->dSites      = DeviceBuffer { ( n + 6 ) * sizeof( Real4 ), false };
+        context.sites     = this->dSites.template get<Real4>();
+        context.minRadius = this->m_minRadius;
+        context.maxRadius = this->m_maxRadius;
+        this->dStatus     = { n * sizeof( uint8_t ), true };
+        context.status    = this->dStatus.template get<uint8_t>();
+        this->dVertices   = DeviceBuffer { sizeof( Vertex ) * 152 * std::size_t( n ), false };
+        this->dVerticesNb = DeviceBuffer { sizeof( uint32_t ) * n, true };
+        context.vertexNb  = this->dVerticesNb.template get<uint32_t>();
+        context.vertices  = this->dVertices.template get<Vertex>();
+        this->dEdges      = DeviceBuffer { sizeof( Edge ) * 264 * std::size_t( n ), false };
+        this->dEdgesNb    = DeviceBuffer { sizeof( uint32_t ) * n, true };
+        context.edges     = this->dEdges.template get<Edge>();
+        context.edgeNb    = this->dEdgesNb.template get<uint32_t>();
+
+        // sites, then the six joggled bounding sites around the box centre
+        mmemcpy<MemcpyType::HostToDevice>( this->dSites.template get<Real>(), this->m_sites.ptr, this->m_sites.size );
+        {
+            const Real cx = ( this->m_minX + this->m_maxX ) / Real( 2 ), cy = ( this->m_minY + this->m_maxY ) / Real( 2 ),
+                       cz = ( this->m_minZ + this->m_maxZ ) / Real( 2 );
+            const Real3 centre { cx, cy, cz };
+            const Real  aabbRadius = apo::gpu::stagedLength( centre - Real3 { this->m_maxX, this->m_maxY, this->m_maxZ } );
+            const Real  radius     = aabbRadius * ( std::sqrt( Real( 3. ) ) + Real( 1e-1 ) );
+            const Real  r0         = context.minRadius;
+            std::vector<Real4> art = {
+                Real4 { cx + radius, cy + Real( 0 ), cz + Real( 0 ), Real( 0 ) + r0 },
+                Real4 { cx - radius, cy + Real( 0 ), cz + Real( 0 ), Real( 0 ) + r0 },
+                Real4 { cx + Real( 0 ), cy + radius, cz + Real( 0 ), Real( 0 ) + r0 },
+                Real4 { cx + Real( 0 ), cy - radius, cz + Real( 0 ), Real( 0 ) + r0 },
+                Real4 { cx + Real( 0 ), cy + Real( 0 ), cz + radius, Real( 0 ) + r0 },
+                Real4 { cx + Real( 0 ), cy + Real( 0 ), cz - radius, Real( 0 ) + r0 },
+            };
+            apo::joggle( { reinterpret_cast<Real *>( art.data() ), 6 * 4 }, 1e-1 );
+            mmemcpy<MemcpyType::HostToDevice>( this->dSites.template get<Real4>() + n, art.data(), 6 );
+        }
+        // initial cell: 8 vertices and 12 edges on the bounding sites
+        std::vector<uint32_t> init;
+        const uint32_t vt[ 8 ][ 3 ] = { { 0, 2, 4 }, { 0, 2, 5 }, { 0, 3, 4 }, { 0, 3, 5 }, { 1, 2, 4 }, { 1, 2, 5 }, { 1, 3, 4 }, { 1, 3, 5 } };
+        const uint32_t et[ 12 ][ 2 ] = { { 0, 2 }, { 2, 4 }, { 1, 2 }, { 2, 5 }, { 1, 4 }, { 1, 5 }, { 0, 5 }, { 0, 4 }, { 1, 3 }, { 3, 5 }, { 0, 3 }, { 3, 4 } };
+        for ( auto & v : vt )
+            init.insert( init.end(), { n + v[ 0 ], n + v[ 1 ], n + v[ 2 ], 0u } );
+        for ( auto & e : et )
+            init.insert( init.end(), { n + e[ 0 ], n + e[ 1 ] } );
+        DeviceBuffer initData = DeviceBuffer::Typed<uint32_t>( init.size() );
+        mmemcpy<MemcpyType::HostToDevice>( initData.template get<uint32_t>(), init.data(), init.size() );
+
+        Aabbf aabb = { make_float3( this->m_minX, this->m_minY, this->m_minZ ), make_float3( this->m_maxX, this->m_maxY, this->m_maxZ ) };
+        this->bvh  = LBVH {};
+        this->bvh.build( n, aabb, context.sites );
+
+        auto [ gridDim, blockDim ] = KernelConfig::From( n, impl::KnnBlockSize );
+        initializeDataStructure<impl::TotalMaxVertexNb, impl::TotalMaxEdgeNb><<<gridDim, blockDim>>>(
+            context, initData.template get<uint32_t>(), initData.template get<uint32_t>() + 32 );
+        check( "initializeDataStructure" );
+
+        DeviceBuffer knns = DeviceBuffer( n * K * ( sizeof( uint32_t ) + sizeof( Real ) ), false );
+        cudaMemset( knns.template get<uint32_t>(), 0xff, sizeof( uint32_t ) * n * K );
+        std::vector<float> lowest( n, std::numeric_limits<float>::lowest() );
+        DeviceBuffer       knownRadii = DeviceBuffer::Typed<float>( n, false );
+        mmemcpy<MemcpyType::HostToDevice>( knownRadii.template get<float>(), lowest.data(), n );
+        for ( uint32_t step = 0; step < this->knnValidationStep; step++ )
+        {
+            impl::getKnns<K><<<gridDim, blockDim>>>( step, context, this->bvh.getDeviceView(), knns.template get<uint32_t>() );
+            auto [ cg, cb ] = KernelConfig::From( n * WarpSize, impl::BlockSize );
+            impl::getCells<<<cg, cb>>>( context, K, knns.template get<uint32_t>(), knownRadii.template get<float>() );
+        }
+        dump( dir, "s1", knownRadii.template get<float>() );
+
+        uint32_t taskNb = thrust::count( thrust::device, context.status, context.status + n, CellStatus::InValidation );
+        for ( uint32_t round = 0; round < 10 && taskNb != 0; round++ )
+        {
+            DeviceBuffer tasks = DeviceBuffer::Typed<uint32_t>( taskNb );
+            thrust::copy_if( thrust::device, thrust::make_counting_iterator<uint32_t>( 0 ),
+                             thrust::make_counting_iterator<uint32_t>( n ), context.status, tasks.template get<uint32_t>(),
+                             thrust::placeholders::_1 == 0 );
+            auto [ cg, cb ] = KernelConfig::From( taskNb * WarpSize, impl::BlockSize );
+            impl::globalVertexValidation<<<cg, cb>>>( context, this->bvh.getDeviceView(), taskNb, tasks.template get<uint32_t>(),
+                                                      knownRadii.template get<float>() );
+            dump( dir, "v" + std::to_string( round ), knownRadii.template get<float>() );
+            impl::globalEdgeValidation<<<cg, cb>>>( context, this->bvh.getDeviceView(), taskNb, tasks.template get<uint32_t>(),
+                                                    knownRadii.template get<float>() );
+            dump( dir, "e" + std::to_string( round ), knownRadii.template get<float>() );
+            taskNb = thrust::count( thrust::device, context.status, context.status + n, uint8_t( 0 ) );
+        }
+        auto [ cg, cb ] = KernelConfig::From( n * WarpSize, impl::BlockSize );
+        impl::globalBisectorValidation<<<cg, cb>>>( context, this->bvh.getDeviceView(), knownRadii.template get<float>() );
+        dump( dir, "b", knownRadii.template get<float>() );
+    }
+};
 
 template<uint32_t K>
 void runReference( std::vector<apo::Real> & sites, const uint32_t n, const std::string & outDir, const int repeat,
@@ -209,7 +350,7 @@ int main( int argc, char ** argv )
 {
     if ( argc < 3 )
     {
-        std::fprintf( stderr, "usage: %s sites.f32 outdir [--time R] [--no-dump] [--k 1|4|8|16] [--knn-steps S]\n", argv[ 0 ] );
+        std::fprintf( stderr, "usage: %s sites.f32 outdir [--time R] [--no-dump] [--k 1|4|8|16] [--knn-steps S] [--stages]\n", argv[ 0 ] );
         return 1;
     }
     const std::string input  = argv[ 1 ];
@@ -218,6 +359,7 @@ int main( int argc, char ** argv )
     bool              dump   = true;
     uint32_t          k        = 16; // AlgorithmGPU<K>
     uint32_t          knnSteps = 1;  // knnValidationStep
+    bool              staged   = false;
     for ( int a = 3; a < argc; a++ )
     {
         if ( !std::strcmp( argv[ a ], "--time" ) && a + 1 < argc )
@@ -228,6 +370,8 @@ int main( int argc, char ** argv )
             k = uint32_t( std::atoi( argv[ ++a ] ) );
         else if ( !std::strcmp( argv[ a ], "--knn-steps" ) && a + 1 < argc )
             knnSteps = uint32_t( std::atoi( argv[ ++a ] ) );
+        else if ( !std::strcmp( argv[ a ], "--stages" ) )
+            staged = true;
     }
 
     // Sites are stored as float32 (x, y, z, r); the reference's FP64 build reads `double`.
@@ -249,6 +393,15 @@ int main( int argc, char ** argv )
 
     std::string json = "{\"n\": " + std::to_string( n );
     json += ", \"k\": " + std::to_string( k ) + ", \"knn_steps\": " + std::to_string( knnSteps );
+    if ( staged )
+    {
+        if ( k != 16 )
+            return 1;
+        StagedBuild<16> algorithm { apo::ConstSpan<apo::Real> { sites.data(), sites.size() }, knnSteps };
+        algorithm.stagedBuild( outDir );
+        std::puts( "staged dumps written" );
+        return 0;
+    }
     switch ( k )
     {
     case 1: runReference<1>( sites, n, outDir, repeat, dump, knnSteps, json ); break;

@@ -44,6 +44,11 @@ CASES = {
     "uni2k_k4s3": ("uniform_cloud(2000, 58.48, 1.5, 0.5)", True, 4, 3),
     "prec1_k8s0": ("precision_cloud(1)", True, 8, 0),
     "prec2_k1s4": ("precision_cloud(2)", True, 1, 4),
+    "uni2k_s0": ("uniform_cloud(2000, 58.48, 1.5, 0.5)", True, 16, 0),
+    # the bench's protein-like packing and the near-degenerate lattices at small sizes
+    "protein20k": ("protein_chains(40, 500, 0.01, seed=3)", False),
+    "latticeA20": ("lattice(20, 'A', seed=4)", False),
+    "latticeB20": ("lattice(20, 'B', seed=5)", False),
 }
 
 

