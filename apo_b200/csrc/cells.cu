@@ -868,6 +868,7 @@ namespace apo2
         uint32_t       err   = 0;
         const uint32_t count = *task_count;
         const uint32_t n     = c.n;
+        const float    rmax  = float( c.scene->rmax );
         for ( uint32_t t = gwarp; t < count; t += nwarp )
         {
             const uint32_t i      = tasks[ t ];
@@ -902,78 +903,102 @@ namespace apo2
                 }
                 const float4 fc = to_float( cur );
 
-                // nearest admissible site to the vertex sphere
-                uint2    stack[ kStack ];
-                int      sp       = 0;
-                uint32_t node     = 0;
-                float    best     = FLT_MAX;
-                uint32_t neighbor = kNone;
-                bool     walking  = need;
-                uint32_t walk_steps = 0;
-                while ( true )
+                // Nearest admissible site to the vertex sphere, in up to two passes. The vertex
+                // only changes when that site conflicts with it (FP64 sphere distance below
+                // 1e-8); a site whose single-precision distance d is above `bound` cannot
+                // conflict (the float distance is within ~1e-6 relative of the double one).
+                // Pass 0 searches from best = bound instead of +inf. A box's distance is at most
+                // max(d, -w) for every site it holds, so every ancestor of a site with
+                // d < bound is entered while best stays at bound: if pass 0 finds no site, none
+                // conflicts and the reference's nearest (whatever it is) leaves the vertex valid.
+                // If it finds one with d > -w, no site holds the vertex centre, box distances
+                // bound every leaf below them, and both searches are exact nearest searches in
+                // the same walk order: same site. Only when the nearest holds the vertex centre
+                // (d <= -w) can the reference's answer depend on its visiting history; pass 1
+                // then repeats its search from +inf for those lanes.
+                const float scale = 1e-5f * ( fabsf( fc.x ) + fabsf( fc.y ) + fabsf( fc.z ) + fabsf( fc.w ) + rmax );
+                const float bound = 1e-2f + scale + fmaxf( 0.f, -fc.w );
+                const float deep  = -fc.w + 1e-3f + scale;
+                uint32_t    neighbor  = kNone;
+                bool        searching = need;
+                for ( uint32_t pass = 0; pass < 2; pass++ )
                 {
-                    if ( walking && ++walk_steps > 4 * n + 64 )
+                    uint2    stack[ kStack ];
+                    int      sp         = 0;
+                    uint32_t node       = 0;
+                    float    best       = pass == 0 ? bound : FLT_MAX;
+                    bool     walking    = searching;
+                    uint32_t walk_steps = 0;
+                    if ( searching )
+                        neighbor = kNone;
+                    while ( true )
                     {
-                        err |= kErrWalk;
-                        walking = false;
-                    }
-                    while ( walking && node < n - 1 )
-                    {
-                        Box      lb, rb;
-                        uint32_t lc, rc;
-                        load_node( c.nodes, node, lb, rb, lc, rc );
-                        const float    dL = lb.distance( fc ), dR = rb.distance( fc );
-                        const bool     leftClosest = dL < dR;
-                        const float    minFar = leftClosest ? dR : dL, minClose = leftClosest ? dL : dR;
-                        const uint32_t farChild = leftClosest ? rc : lc, closeChild = leftClosest ? lc : rc;
-                        const bool     exploreFar = minFar < best, exploreClose = minClose < best;
-                        if ( !exploreFar && !exploreClose )
-                            break;
-                        node = exploreClose ? closeChild : farChild;
-                        if ( exploreClose && exploreFar )
+                        if ( walking && ++walk_steps > 4 * n + 64 )
                         {
-                            if ( sp < int( kStack ) )
-                                stack[ sp++ ] = make_uint2( farChild, __float_as_uint( minFar ) );
-                            else
-                                err |= kErrStack;
-                        }
-                    }
-                    const uint32_t j   = node - ( n - 1 );
-                    bool           can = walking && node >= n - 1 && node < 2 * n - 1 && j != i && j != vx.x && j != vx.y
-                                 && j != vx.z && c.status[ j ] != kBuried;
-                    uint32_t cm = __ballot_sync( kFull, can );
-                    while ( cm )
-                    {
-                        const uint32_t t2 = highest( cm );
-                        cm &= ~( 1u << t2 );
-                        const uint32_t tj     = __shfl_sync( kFull, j, t2 );
-                        const bool     known2 = is_known( w, tj );
-                        if ( lane == t2 )
-                            can = !known2;
-                    }
-                    if ( can )
-                    {
-                        const float d = sphere_distance( c.sites_f[ j ], fc );
-                        if ( d < best )
-                        {
-                            best     = d;
-                            neighbor = j;
-                        }
-                    }
-                    while ( walking )
-                    {
-                        if ( sp == 0 )
-                        {
+                            err |= kErrWalk;
                             walking = false;
+                        }
+                        while ( walking && node < n - 1 )
+                        {
+                            Box      lb, rb;
+                            uint32_t lc, rc;
+                            load_node( c.nodes, node, lb, rb, lc, rc );
+                            const float    dL = lb.distance( fc ), dR = rb.distance( fc );
+                            const bool     leftClosest = dL < dR;
+                            const float    minFar = leftClosest ? dR : dL, minClose = leftClosest ? dL : dR;
+                            const uint32_t farChild = leftClosest ? rc : lc, closeChild = leftClosest ? lc : rc;
+                            const bool     exploreFar = minFar < best, exploreClose = minClose < best;
+                            if ( !exploreFar && !exploreClose )
+                                break;
+                            node = exploreClose ? closeChild : farChild;
+                            if ( exploreClose && exploreFar )
+                            {
+                                if ( sp < int( kStack ) )
+                                    stack[ sp++ ] = make_uint2( farChild, __float_as_uint( minFar ) );
+                                else
+                                    err |= kErrStack;
+                            }
+                        }
+                        const uint32_t j   = node - ( n - 1 );
+                        bool           can = walking && node >= n - 1 && node < 2 * n - 1 && j != i && j != vx.x && j != vx.y
+                                     && j != vx.z && c.status[ j ] != kBuried;
+                        uint32_t cm = __ballot_sync( kFull, can );
+                        while ( cm )
+                        {
+                            const uint32_t t2 = highest( cm );
+                            cm &= ~( 1u << t2 );
+                            const uint32_t tj     = __shfl_sync( kFull, j, t2 );
+                            const bool     known2 = is_known( w, tj );
+                            if ( lane == t2 )
+                                can = !known2;
+                        }
+                        if ( can )
+                        {
+                            const float d = sphere_distance( c.sites_f[ j ], fc );
+                            if ( d < best )
+                            {
+                                best     = d;
+                                neighbor = j;
+                            }
+                        }
+                        while ( walking )
+                        {
+                            if ( sp == 0 )
+                            {
+                                walking = false;
+                                break;
+                            }
+                            --sp;
+                            if ( __uint_as_float( stack[ sp ].y ) > best )
+                                continue;
+                            node = stack[ sp ].x;
                             break;
                         }
-                        --sp;
-                        if ( __uint_as_float( stack[ sp ].y ) > best )
-                            continue;
-                        node = stack[ sp ].x;
-                        break;
+                        if ( !__any_sync( kFull, walking ) )
+                            break;
                     }
-                    if ( !__any_sync( kFull, walking ) )
+                    searching = searching && neighbor != kNone && best <= deep;
+                    if ( !__any_sync( kFull, searching ) )
                         break;
                 }
 
