@@ -378,6 +378,7 @@ apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_
     total += align256( 4 * size_t( n ) ) + align256( 4 * 64 ) + align256( 4 );
     total += align256( 4 * size_t( n ) ) * 2 + align256( 4 * scanWords * 2 ) + align256( 16 );
     total += align256( spec_bytes( n ) );
+    total += align256( walk_scratch_bytes() );
     h->arena.size = total;
     cudaError_t err = cudaMalloc( reinterpret_cast<void **>( &h->arena.base ), total );
     if ( err != cudaSuccess )
@@ -428,6 +429,7 @@ apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_
     h->out.tile_sums  = a.take<uint32_t>( scanWords * 2 );
     h->out.totals     = a.take<uint64_t>( 2 );
     spec_carve( h->spec, a.take<char>( spec_bytes( n ) ), n );
+    c.walk_scratch    = a.take<uint32_t>( walk_scratch_bytes() / sizeof( uint32_t ) );
     sort_scratch_carve( h->sort, sortBase, n, h->error );
     if ( a.used > a.size )
     {

@@ -1038,6 +1038,170 @@ namespace apo2
     // while the cell's neighbours still include all of U0 (updates only added some), an edge
     // with no contributor then has none now: its search would find nothing and is skipped.
     // Once a neighbour of U0 has left the cell, every edge is searched again.
+    // One edge's contributor search in the exact edge pass: the bounding volume of the
+    // trisector and the ball its contributors must reach (see k_edge_validation).
+    struct EdgeWalk
+    {
+        float4   bsph, reach;
+        float3   n1, n2, pp1, pp2;
+        bool     hyperbola;
+        uint32_t k, l;
+        double4  sk, sl;
+    };
+
+    __device__ __forceinline__ float3 shfl3( float3 v, uint32_t src )
+    {
+        return make_float3( __shfl_sync( kFull, v.x, src ), __shfl_sync( kFull, v.y, src ), __shfl_sync( kFull, v.z, src ) );
+    }
+    __device__ __forceinline__ float4 shfl4f( float4 v, uint32_t src )
+    {
+        return make_float4( __shfl_sync( kFull, v.x, src ), __shfl_sync( kFull, v.y, src ), __shfl_sync( kFull, v.z, src ),
+                            __shfl_sync( kFull, v.w, src ) );
+    }
+
+    // Lane-local forms of is_known / edges_clear (same predicates, one lane scanning all edges).
+    __device__ __forceinline__ bool known_by_lane( const WarpCell & w, uint32_t id )
+    {
+        for ( uint32_t e = 0; e < w.en; e++ )
+        {
+            const uint4 r = w.e[ e ];
+            if ( r.x == id || r.y == id )
+                return true;
+        }
+        return false;
+    }
+    __device__ __forceinline__ bool clear_by_lane( const CellContext & c, const WarpCell & w, double4 sphere, uint32_t skip1,
+                                                   uint32_t skip2 )
+    {
+        for ( uint32_t e = 0; e < w.en; e++ )
+        {
+            const uint4 r = w.e[ e ];
+            if ( r.x != skip1 && r.x != skip2 && intersects( site( c, r.x ), sphere ) )
+                return false;
+            if ( r.y != skip1 && r.y != skip2 && intersects( site( c, r.y ), sphere ) )
+                return false;
+        }
+        return true;
+    }
+
+    // The rest of a long edge search, walked by the whole warp in the lane walk's order.
+    // The walk has no running bound: which children of a node are entered, and in which order
+    // (closer first), depends on the node alone, so its leaves come in one fixed order and the
+    // answer is the first contributing leaf of that order. The frontier (nodes not yet expanded,
+    // in that order) is a stack in `frontier`, its earliest node on top. Each step expands the
+    // 32 earliest nodes at once: an internal node is replaced by its entered children, a leaf
+    // is tested. When the earliest contributing leaf of a step sits at position q, the answer
+    // is it or a leaf under one of the q nodes before it: everything after it is dropped and
+    // the walk continues over those. `saved` holds the suspended lane's position (its current
+    // node, then its stack from the top), `count` entries, earliest first.
+    __device__ uint32_t ordered_edge_walk( const CellContext & c, const WarpCell & w, uint32_t i, double4 si, const EdgeWalk & p,
+                                           uint32_t * frontier, const uint32_t * saved, uint32_t count, uint32_t & err )
+    {
+        const uint32_t lane = lane_id();
+        const uint32_t n    = c.n;
+        for ( uint32_t q = lane; q < count; q += 32 )
+            frontier[ count - 1 - q ] = saved[ q ];
+        __syncwarp();
+        uint32_t top = count, found = kNone, steps = 0;
+        while ( top > 0 )
+        {
+            if ( ++steps > 4 * n + 64 )
+            {
+                err |= kErrWalk;
+                break;
+            }
+            const uint32_t m    = min( 32u, top );
+            const uint32_t node = lane < m ? frontier[ top - 1 - lane ] : kNone;
+            __syncwarp();
+            uint32_t first = 0, second = 0, kids = 0;
+            bool     contrib = false;
+            uint32_t j       = kNone;
+            if ( lane < m && node < n - 1 )
+            {
+                Box      lb, rb;
+                uint32_t lc, rc;
+                load_node( c.nodes, node, lb, rb, lc, rc );
+                const float3   closeL = lb.closest( p.bsph ), closeR = rb.closest( p.bsph );
+                const float    dL = lb.distance( p.bsph ), dR = rb.distance( p.bsph );
+                const bool     leftClosest = dL < dR;
+                const float    minFar = leftClosest ? dR : dL, minClose = leftClosest ? dL : dR;
+                const float3   farPoint = leftClosest ? closeR : closeL, closePoint = leftClosest ? closeL : closeR;
+                const uint32_t farChild = leftClosest ? rc : lc, closeChild = leftClosest ? lc : rc;
+                bool           exploreFar = minFar < 0.f;
+                if ( p.hyperbola && exploreFar )
+                    exploreFar = fdot( p.n1, farPoint - p.pp1 ) < 0.f && fdot( p.n2, farPoint - p.pp2 ) < 0.f;
+                bool exploreClose = minClose < 0.f;
+                if ( p.hyperbola && exploreClose )
+                    exploreClose = fdot( p.n1, closePoint - p.pp1 ) < 0.f && fdot( p.n2, closePoint - p.pp2 ) < 0.f;
+                exploreFar   = exploreFar && ( leftClosest ? rb : lb ).distance( p.reach ) < 0.f;
+                exploreClose = exploreClose && ( leftClosest ? lb : rb ).distance( p.reach ) < 0.f;
+                if ( exploreClose )
+                {
+                    first = closeChild;
+                    kids  = 1;
+                    if ( exploreFar )
+                    {
+                        second = farChild;
+                        kids   = 2;
+                    }
+                }
+                else if ( exploreFar )
+                {
+                    first = farChild;
+                    kids  = 1;
+                }
+            }
+            else if ( lane < m && node < 2 * n - 1 )
+            {
+                j       = node - ( n - 1 );
+                bool can = j != i && j != p.k && j != p.l && c.status[ j ] != kBuried;
+                double4 sj = make_double4( 0, 0, 0, 0 );
+                if ( can )
+                {
+                    sj              = c.sites[ j ];
+                    const float4 fj = to_float( sj );
+                    can             = intersects( fj, p.bsph ) && flength( f3( fj ) - f3( p.reach ) ) <= p.reach.w;
+                    if ( p.hyperbola )
+                        can = can && double( fdot( p.n1, f3( fj ) - p.pp1 ) ) < -sj.w
+                              && double( fdot( p.n2, f3( fj ) - p.pp2 ) ) < -sj.w;
+                }
+                if ( can )
+                    can = !known_by_lane( w, j );
+                if ( can )
+                {
+                    double4 x0 = make_double4( 0, 0, 0, 0 ), x1 = make_double4( 0, 0, 0, 0 );
+                    const uint32_t mask = quadrisector( si, sj, p.sk, p.sl, x0, x1 );
+                    contrib = mask == 3 && ( clear_by_lane( c, w, x0, p.k, p.l ) || clear_by_lane( c, w, x1, p.k, p.l ) );
+                }
+            }
+            const uint32_t hits = __ballot_sync( kFull, contrib );
+            uint32_t       keep = m, base = top - m;
+            if ( hits )
+            {
+                const uint32_t q = __ffs( hits ) - 1;
+                found            = __shfl_sync( kFull, j, q );
+                keep             = q;
+                base             = 0;
+            }
+            const uint32_t mine  = lane < keep ? kids : 0u;
+            uint32_t       total = 0;
+            const uint32_t off   = warp_exclusive_scan( mine, total );
+            if ( base + total > kCoopCap )
+            {
+                err |= kErrStack;
+                break;
+            }
+            // the earliest child ends on top
+            if ( mine >= 1 )
+                frontier[ base + total - 1 - off ] = first;
+            if ( mine == 2 )
+                frontier[ base + total - 2 - off ] = second;
+            __syncwarp();
+            top = base + total;
+        }
+        return found;
+    }
+
     __global__ void __launch_bounds__( kCellBlock, 4 ) k_edge_validation( CellContext c, const uint32_t * __restrict__ tasks,
                                                                       const uint32_t * __restrict__ task_count,
                                                                       SearchProof proof )
@@ -1051,6 +1215,8 @@ namespace apo2
         uint32_t       err   = 0;
         const uint32_t count = *task_count;
         const uint32_t n     = c.n;
+        uint32_t *     frontier = c.walk_scratch + size_t( gwarp ) * kWalkScratchWords;
+        uint32_t *     saved    = frontier + kCoopCap + lane * ( kStack + 1 );
         for ( uint32_t t = gwarp; t < count; t += nwarp )
         {
             const uint32_t i      = tasks[ t ];
@@ -1187,12 +1353,25 @@ namespace apo2
                 uint32_t found   = kNone;
                 bool     walking = need && !skip;
                 uint32_t walk_steps = 0;
+                bool     suspended  = false;
+                uint32_t saved_count = 0;
                 while ( true )
                 {
                     if ( walking && ++walk_steps > 4 * n + 64 )
                     {
                         err |= kErrWalk;
                         walking = false;
+                    }
+                    if ( walking && walk_steps > kLaneWalk )
+                    {
+                        // a long search: its position (current node, then the stack from the
+                        // top) goes to scratch and the warp finishes it below
+                        saved[ 0 ] = node;
+                        for ( int q = 0; q < sp; q++ )
+                            saved[ 1 + q ] = stack[ sp - 1 - q ];
+                        saved_count = uint32_t( sp ) + 1;
+                        suspended   = true;
+                        walking     = false;
                     }
                     while ( walking && node < n - 1 )
                     {
@@ -1287,6 +1466,30 @@ namespace apo2
                     }
                     if ( !__any_sync( kFull, walking ) )
                         break;
+                }
+                __syncwarp();
+                uint32_t pending = __ballot_sync( kFull, suspended );
+                while ( pending )
+                {
+                    const uint32_t src = __ffs( pending ) - 1;
+                    pending &= pending - 1;
+                    EdgeWalk p;
+                    p.bsph      = shfl4f( bsph, src );
+                    p.reach     = shfl4f( reach, src );
+                    p.n1        = shfl3( n1, src );
+                    p.n2        = shfl3( n2, src );
+                    p.pp1       = shfl3( pp1, src );
+                    p.pp2       = shfl3( pp2, src );
+                    p.hyperbola = __shfl_sync( kFull, int( hyperbola ), src ) != 0;
+                    p.k         = __shfl_sync( kFull, k, src );
+                    p.l         = __shfl_sync( kFull, l, src );
+                    p.sk        = shfl4( sk, src );
+                    p.sl        = shfl4( sl, src );
+                    const uint32_t cnt = __shfl_sync( kFull, saved_count, src );
+                    const uint32_t got = ordered_edge_walk( c, w, i, si, p, frontier,
+                                                            frontier + kCoopCap + src * ( kStack + 1 ), cnt, err );
+                    if ( lane == src )
+                        found = got;
                 }
                 if ( need && found == kNone )
                     w.e[ eid ].w = ( w.e[ eid ].w & 0xffffff00u ) | 1u;
@@ -1830,6 +2033,12 @@ namespace apo2
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_cells, kCellBlock, cell_smem_bytes( false ) );
         g_cell_grid = sms * std::max( 1, per_sm );
+    }
+
+    size_t walk_scratch_bytes()
+    {
+        configure_cell_kernels();
+        return size_t( g_cell_grid ) * ( kCellBlock / 32 ) * kWalkScratchWords * sizeof( uint32_t );
     }
 
     static int cell_grid( uint32_t cells )

@@ -39,7 +39,15 @@ namespace apo2
         uint4 *          edges       = nullptr; // n * 264 records (j, k, vertex count, status)
         uint32_t *       error       = nullptr;
         const Scene *    scene       = nullptr; // bounds and radius range of the sites
+        uint32_t *       walk_scratch = nullptr; // kWalkScratchWords per warp of the exact edge pass
     };
+
+    // Exact edge validation: a lane walks its edge's search alone for kLaneWalk steps; a
+    // search still running then is finished by the whole warp, in the same order, from a
+    // frontier of at most kCoopCap nodes kept in global scratch (plus each lane's saved stack).
+    constexpr uint32_t kLaneWalk         = 256;
+    constexpr uint32_t kCoopCap          = 4096;
+    constexpr uint32_t kWalkScratchWords = kCoopCap + 32 * ( kStack + 1 );
 
     // Position of a stored vertex: root `type` of quadrisector(si, sj, sk, sl) with the
     // sorted ids (topology_update.inl:104-111).
@@ -84,6 +92,8 @@ namespace apo2
         return float( r ) * 1.0001f + 1e-3f;
     }
     void configure_cell_kernels();
+    // bytes of CellContext::walk_scratch: one region per warp the cell kernels launch
+    size_t walk_scratch_bytes();
     // k_cells modes: first kNN step, a later kNN step, initial cells only (no kNN step)
     constexpr uint32_t kCellsFirst    = 0;
     constexpr uint32_t kCellsNext     = 1;
