@@ -103,7 +103,7 @@ namespace apo2
     void launch_tasks( const CellContext & c, uint32_t * tasks, uint32_t * count, cudaStream_t s );
     void launch_vertex_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s );
     constexpr uint32_t kMaybeWords = ( kMaxEdges + 31 ) / 32; // 9 words of edge bits per task
-    constexpr uint32_t kNbrCap     = 64;                      // neighbour slots per task cell
+    constexpr uint32_t kNbrCap     = 272;                     // neighbour slots per task cell (>= the 265 a full cell can have)
 
     // What the edge-parallel search proved, handed to the exact pass of the same cells.
     struct SearchProof

@@ -638,7 +638,8 @@ namespace apo2
         }
     }
 
-    static size_t heavy_capacity( uint32_t n ) { return size_t( n ) + 1024; }
+    // long lane searches per round: log-normal radii reach 1.5 per site
+    static size_t heavy_capacity( uint32_t n ) { return 6 * size_t( n ) + 65536; }
     static size_t sub_capacity( uint32_t n ) { return 4 * size_t( n ) + 65536; }
 
     size_t spec_bytes( uint32_t n )
