@@ -333,9 +333,9 @@ namespace apo2
                         s.t              = lo;
                         const uint32_t e = uint32_t( item - b.item_offset[ s.t ] );
                         s.e              = e;
-                        if ( b.cell_flag[ s.t ] )
+                        if ( b.cell_flag[ s.t ] & kFlagOverflow )
                         {
-                            // the cell goes to the exact path anyway; leave this edge undecided there
+                            // no neighbour list for this cell: the exact path searches this edge
                             atomicOr( &b.maybe_bits[ size_t( s.t ) * kMaybeWords + ( e >> 5 ) ], 1u << ( e & 31 ) );
                         }
                         else
@@ -530,9 +530,10 @@ namespace apo2
             if ( item >= count )
                 break;
             const uint2 h = b.heavy[ item ];
-            if ( b.cell_flag[ h.x ] )
+            // Edges of a cell that already goes to the exact path are still searched: every
+            // edge proven empty here is one the exact pass skips.
+            if ( b.cell_flag[ h.x ] & kFlagOverflow )
             {
-                // undecided edge of a cell that goes to the exact path: search it there
                 if ( lane == 0 )
                     atomicOr( &b.maybe_bits[ size_t( h.x ) * kMaybeWords + ( h.y >> 5 ) ], 1u << ( h.y & 31 ) );
                 continue;
@@ -582,7 +583,9 @@ namespace apo2
                 break;
             const uint2 sub = b.sub[ q ];
             const uint2 h   = b.heavy[ sub.x ];
-            if ( b.cell_flag[ h.x ] )
+            // another part of this edge's search already found a contributor
+            if ( ( b.cell_flag[ h.x ] & kFlagOverflow )
+                 || ( ( b.maybe_bits[ size_t( h.x ) * kMaybeWords + ( h.y >> 5 ) ] >> ( h.y & 31 ) ) & 1u ) )
             {
                 if ( lane == 0 )
                     atomicOr( &b.maybe_bits[ size_t( h.x ) * kMaybeWords + ( h.y >> 5 ) ], 1u << ( h.y & 31 ) );
