@@ -93,6 +93,9 @@ SIGNATURES = {
     "apo2_radix_sort_pairs": (_I, [_P, _P, _U32, _P, _P]),
     "apo2_radix_sort_pairs_static": (_I, [_P, _P, _U32, _P]),
     "apo2_generate_chains": (_I, [_U32, _U32, ctypes.c_double, _U64, _P]),
+    "apo2_batch_create": (_I, [_U32, _U32, _P, _P]),
+    "apo2_batch_build": (_I, [_P, _P, _P, _U32, _P, _P, _P, _P]),
+    "apo2_batch_destroy": (_I, [_P]),
 }
 
 
@@ -267,6 +270,57 @@ class AlgorithmGPU:
         s = Stats()
         _check(self._lib.apo2_get_stats(self._h, ctypes.byref(s)))
         return s.as_dict()
+
+
+class Batch:
+    """Many independent diagrams of uneven size per call (apo2_batch_*): `streams` workers, each
+    with device memory for `max_sites` sites, build the diagrams largest first, overlapping."""
+
+    def __init__(self, max_sites: int, streams: int = 8, k: int = 16, device: int = 0):
+        lib = load_library()
+        opt = Options()
+        opt.struct_size = ctypes.sizeof(Options)
+        opt.k = k
+        opt.device = device
+        handle = ctypes.c_void_p()
+        _check(lib.apo2_batch_create(max_sites, streams, ctypes.byref(opt), ctypes.byref(handle)))
+        self._b = handle
+        self._lib = lib
+
+    def build(self, diagrams, vertices: bool = True):
+        """diagrams: list of (n_i, 4) float32 arrays. Returns (list of VertexDiagram or None,
+        per-diagram vertex counts, per-diagram device ms)."""
+        arrays = [np.ascontiguousarray(np.asarray(d, dtype=np.float32).reshape(-1, 4)) for d in diagrams]
+        offsets = np.zeros(len(arrays) + 1, dtype=np.uint64)
+        offsets[1:] = np.cumsum([a.shape[0] for a in arrays])
+        sites = np.ascontiguousarray(np.concatenate(arrays, axis=0)) if arrays else np.zeros((0, 4), np.float32)
+        voff = np.zeros(len(arrays) + 1, dtype=np.uint64)
+        ms = np.zeros(len(arrays), dtype=np.float32)
+        pos, ids = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(self._lib.apo2_batch_build(self._b, sites.ctypes.data, offsets.ctypes.data, len(arrays), voff.ctypes.data,
+                                          ctypes.byref(pos) if vertices else None, ctypes.byref(ids) if vertices else None,
+                                          ms.ctypes.data))
+        counts = np.diff(voff).astype(np.int64)
+        out = None
+        if vertices:
+            total = int(voff[-1])
+            try:
+                P = np.ctypeslib.as_array(ctypes.cast(pos, ctypes.POINTER(ctypes.c_double)), shape=(max(total, 1) * 4,))[:total * 4].copy()
+                I = np.ctypeslib.as_array(ctypes.cast(ids, ctypes.POINTER(ctypes.c_uint32)), shape=(max(total, 1) * 4,))[:total * 4].copy()
+            finally:
+                self._lib.apo2_free(pos)
+                self._lib.apo2_free(ids)
+            out = [VertexDiagram(vertices=P[4 * int(voff[d]):4 * int(voff[d + 1])], verticesId=I[4 * int(voff[d]):4 * int(voff[d + 1])])
+                   for d in range(len(arrays))]
+        return out, counts, ms
+
+    def close(self):
+        if getattr(self, "_b", None) is not None and self._b.value:
+            self._lib.apo2_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        self.close()
 
 
 def computeApolloniusDiagram(sites) -> VertexDiagram:

@@ -10,6 +10,9 @@
 #include <string>
 #include <tuple>
 #include <vector>
+#include <algorithm>
+#include <atomic>
+#include <thread>
 
 #include "../../include/apo2.h"
 #include "cells.cuh"
@@ -319,6 +322,122 @@ const char * apo2_version( void ) { return "apo2 1.0 (sm_100a)"; }
 
 const char * apo2_last_error_string( void ) { return g_last_error.c_str(); }
 
+namespace
+{
+    // Device bytes of a handle for n sites (every array of the build, carved from one block).
+    size_t arena_bytes( uint32_t n, const apo2_options & opt, bool f64 )
+    {
+        const size_t nodes     = 2 * size_t( n ) - 1;
+        const size_t sortBytes = sort_scratch_bytes( n );
+        const size_t scanWords = output_scan_scratch_words( n );
+        size_t       total     = 0;
+        total += align256( size_t( n ) * ( f64 ? 32 : 16 ) );
+        total += align256( sizeof( double4 ) * n );
+        total += align256( bounds_partial_bytes( 148 * 4 ) ) + align256( 4 ) + align256( sizeof( Scene ) );
+        total += align256( 8 * size_t( n ) ) + align256( 4 * size_t( n ) ) + align256( sizeof( double4 ) * ( n + kArtificial ) )
+                 + align256( sizeof( float4 ) * n ) + 3 * align256( 4 * nodes ) + align256( sizeof( float4 ) * 2 * nodes )
+                 + align256( 4 * nodes ) + align256( 4 * size_t( n ) ) + align256( sizeof( WideNode ) * n );
+        total += align256( sortBytes );
+        total += align256( size_t( n ) ) + align256( 4 * size_t( n ) * opt.k ) + align256( 4 * size_t( n ) ) * 3
+                 + align256( sizeof( uint4 ) * kMaxVertices * size_t( n ) ) + align256( sizeof( uint4 ) * kMaxEdges * size_t( n ) );
+        total += align256( 4 * size_t( n ) ) + align256( 4 * 64 ) + align256( 4 );
+        total += align256( 4 * size_t( n ) ) * 2 + align256( 4 * scanWords * 2 ) + align256( 16 );
+        total += align256( spec_bytes( n ) );
+        total += align256( walk_scratch_bytes() );
+        return total;
+    }
+
+    // Points every array of the handle into its arena for n sites (n at most the size the
+    // arena was allocated for: every array grows with n). Returns false if it does not fit.
+    bool carve( apo2_handle * h, uint32_t n )
+    {
+        const size_t nodes     = 2 * size_t( n ) - 1;
+        const size_t sortBytes = sort_scratch_bytes( n );
+        const size_t scanWords = output_scan_scratch_words( n );
+        const apo2_options & opt = h->options;
+        h->n             = n;
+        h->partial_count = 148 * 4;
+        Arena & a        = h->arena;
+        a.used           = 0;
+        h->input          = a.take<char>( size_t( n ) * ( h->input_f64 ? 32 : 16 ) );
+        h->input_d4       = a.take<double4>( n );
+        h->partials       = reinterpret_cast<BoundsPartial *>( a.take<char>( bounds_partial_bytes( h->partial_count ) ) );
+        h->bounds_counter = a.take<uint32_t>( 1 );
+        h->scene          = a.take<Scene>( 1 );
+        Tree & t          = h->tree;
+        t.codes           = a.take<uint64_t>( n );
+        t.indices         = a.take<uint32_t>( n );
+        t.sites           = a.take<double4>( n + kArtificial );
+        t.sites_f         = a.take<float4>( n );
+        t.parent          = a.take<int32_t>( nodes );
+        t.left            = a.take<int32_t>( nodes );
+        t.right           = a.take<int32_t>( nodes );
+        t.boxes           = a.take<float4>( 2 * nodes );
+        t.sizes           = a.take<uint32_t>( nodes );
+        t.arrivals        = a.take<uint32_t>( n );
+        t.nodes           = a.take<WideNode>( n );
+        void * sortBase   = a.take<char>( sortBytes );
+        CellContext & c   = h->cells;
+        c.n               = n;
+        c.k               = opt.k;
+        c.sites           = t.sites;
+        c.sites_f         = t.sites_f;
+        c.nodes           = t.nodes;
+        c.indices         = t.indices;
+        c.status          = a.take<uint8_t>( n );
+        c.knn             = a.take<uint32_t>( size_t( n ) * opt.k );
+        c.known_radii     = a.take<float>( n );
+        c.vertex_nb       = a.take<uint32_t>( n );
+        c.edge_nb         = a.take<uint32_t>( n );
+        c.vertices        = a.take<uint4>( size_t( n ) * kMaxVertices );
+        c.edges           = a.take<uint4>( size_t( n ) * kMaxEdges );
+        h->tasks          = a.take<uint32_t>( n );
+        h->task_counts    = a.take<uint32_t>( 64 );
+        h->error          = a.take<uint32_t>( 1 );
+        c.error           = h->error;
+        c.scene           = h->scene;
+        h->out.vcount     = a.take<uint32_t>( n );
+        h->out.ccount     = a.take<uint32_t>( n );
+        h->out.tile_sums  = a.take<uint32_t>( scanWords * 2 );
+        h->out.totals     = a.take<uint64_t>( 2 );
+        spec_carve( h->spec, a.take<char>( spec_bytes( n ) ), n );
+        c.walk_scratch    = a.take<uint32_t>( walk_scratch_bytes() / sizeof( uint32_t ) );
+        sort_scratch_carve( h->sort, sortBase, n, h->error );
+        return a.used <= a.size;
+    }
+} // namespace
+
+namespace
+{
+    // Checks the caller's options and fills in the defaults.
+    apo2_status normalize_options( const apo2_options * options, apo2_options & opt )
+    {
+        opt = apo2_options {};
+        if ( options )
+        {
+            if ( options->struct_size != sizeof( apo2_options ) )
+                return fail( APO2_ERR_INVALID_ARG, "apo2_options.struct_size mismatch" );
+            opt = *options;
+        }
+        if ( opt.k == 0 )
+            opt.k = 16;
+        if ( opt.k > kMaxK )
+            return fail( APO2_ERR_INVALID_ARG, "k is at most 16" );
+        if ( opt.max_iterations == 0 )
+            opt.max_iterations = 10;
+        if ( opt.edge_search > 1 )
+            return fail( APO2_ERR_INVALID_ARG, "edge_search is 0 or 1" );
+        if ( opt.knn_steps == 0 )
+            opt.knn_steps = 1;
+        else if ( opt.knn_steps == APO2_NO_KNN_STEPS )
+            opt.knn_steps = 0;
+        else if ( opt.knn_steps > 64 )
+            return fail( APO2_ERR_INVALID_ARG, "knn_steps is at most 64" );
+        opt.max_iterations = std::min( opt.max_iterations, 64u );
+        return APO2_OK;
+    }
+} // namespace
+
 apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_location location, const apo2_options * options,
                          apo2_handle ** out )
 {
@@ -327,28 +446,10 @@ apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_
         return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_create" );
     if ( n > ( 1u << 28 ) )
         return fail( APO2_ERR_TOO_LARGE, "at most 2^28 sites" );
-    apo2_options opt {};
-    if ( options )
-    {
-        if ( options->struct_size != sizeof( apo2_options ) )
-            return fail( APO2_ERR_INVALID_ARG, "apo2_options.struct_size mismatch" );
-        opt = *options;
-    }
-    if ( opt.k == 0 )
-        opt.k = 16;
-    if ( opt.k > kMaxK )
-        return fail( APO2_ERR_INVALID_ARG, "k is at most 16" );
-    if ( opt.max_iterations == 0 )
-        opt.max_iterations = 10;
-    if ( opt.edge_search > 1 )
-        return fail( APO2_ERR_INVALID_ARG, "edge_search is 0 or 1" );
-    if ( opt.knn_steps == 0 )
-        opt.knn_steps = 1;
-    else if ( opt.knn_steps == APO2_NO_KNN_STEPS )
-        opt.knn_steps = 0;
-    else if ( opt.knn_steps > 64 )
-        return fail( APO2_ERR_INVALID_ARG, "knn_steps is at most 64" );
-    opt.max_iterations = std::min( opt.max_iterations, 64u );
+    apo2_options      opt {};
+    const apo2_status ost = normalize_options( options, opt );
+    if ( ost != APO2_OK )
+        return ost;
 
     APO2_CUDA( cudaSetDevice( int( opt.device ) ), "cudaSetDevice" );
     apo2_handle * h = new ( std::nothrow ) apo2_handle {};
@@ -360,80 +461,18 @@ apo2_status apo2_create( const void * sites, uint32_t n, apo2_dtype dtype, apo2_
     h->input_f64 = dtype == APO2_F64;
     configure_cell_kernels();
 
-    // sizes
-    const size_t nodes = 2 * size_t( n ) - 1;
-    h->partial_count   = 148 * 4;
-    const size_t sortBytes = sort_scratch_bytes( n );
-    const size_t scanWords = output_scan_scratch_words( n );
-    size_t       total     = 0;
-    total += align256( size_t( n ) * ( h->input_f64 ? 32 : 16 ) );
-    total += align256( sizeof( double4 ) * n );
-    total += align256( bounds_partial_bytes( h->partial_count ) ) + align256( 4 ) + align256( sizeof( Scene ) );
-    total += align256( 8 * size_t( n ) ) + align256( 4 * size_t( n ) ) + align256( sizeof( double4 ) * ( n + kArtificial ) )
-             + align256( sizeof( float4 ) * n ) + 3 * align256( 4 * nodes ) + align256( sizeof( float4 ) * 2 * nodes )
-             + align256( 4 * nodes ) + align256( 4 * size_t( n ) ) + align256( sizeof( WideNode ) * n );
-    total += align256( sortBytes );
-    total += align256( size_t( n ) ) + align256( 4 * size_t( n ) * opt.k ) + align256( 4 * size_t( n ) ) * 3
-             + align256( sizeof( uint4 ) * kMaxVertices * size_t( n ) ) + align256( sizeof( uint4 ) * kMaxEdges * size_t( n ) );
-    total += align256( 4 * size_t( n ) ) + align256( 4 * 64 ) + align256( 4 );
-    total += align256( 4 * size_t( n ) ) * 2 + align256( 4 * scanWords * 2 ) + align256( 16 );
-    total += align256( spec_bytes( n ) );
-    total += align256( walk_scratch_bytes() );
-    h->arena.size = total;
-    cudaError_t err = cudaMalloc( reinterpret_cast<void **>( &h->arena.base ), total );
+    configure_spec_kernels();
+    const size_t total = arena_bytes( n, opt, h->input_f64 );
+    h->arena.size      = total;
+    cudaError_t err    = cudaMalloc( reinterpret_cast<void **>( &h->arena.base ), total );
     if ( err != cudaSuccess )
     {
         delete h;
         return cuda_fail( err, "device allocation" );
     }
-    Arena & a         = h->arena;
-    h->input          = a.take<char>( size_t( n ) * ( h->input_f64 ? 32 : 16 ) );
-    h->input_d4       = a.take<double4>( n );
-    h->partials       = reinterpret_cast<BoundsPartial *>( a.take<char>( bounds_partial_bytes( h->partial_count ) ) );
-    h->bounds_counter = a.take<uint32_t>( 1 );
-    h->scene          = a.take<Scene>( 1 );
-    Tree & t          = h->tree;
-    t.codes           = a.take<uint64_t>( n );
-    t.indices         = a.take<uint32_t>( n );
-    t.sites           = a.take<double4>( n + kArtificial );
-    t.sites_f         = a.take<float4>( n );
-    t.parent          = a.take<int32_t>( nodes );
-    t.left            = a.take<int32_t>( nodes );
-    t.right           = a.take<int32_t>( nodes );
-    t.boxes           = a.take<float4>( 2 * nodes );
-    t.sizes           = a.take<uint32_t>( nodes );
-    t.arrivals        = a.take<uint32_t>( n );
-    t.nodes           = a.take<WideNode>( n );
-    void * sortBase   = a.take<char>( sortBytes );
-    CellContext & c   = h->cells;
-    c.n               = n;
-    c.k               = opt.k;
-    c.sites           = t.sites;
-    c.sites_f         = t.sites_f;
-    c.nodes           = t.nodes;
-    c.indices         = t.indices;
-    c.status          = a.take<uint8_t>( n );
-    c.knn             = a.take<uint32_t>( size_t( n ) * opt.k );
-    c.known_radii     = a.take<float>( n );
-    c.vertex_nb       = a.take<uint32_t>( n );
-    c.edge_nb         = a.take<uint32_t>( n );
-    c.vertices        = a.take<uint4>( size_t( n ) * kMaxVertices );
-    c.edges           = a.take<uint4>( size_t( n ) * kMaxEdges );
-    h->tasks          = a.take<uint32_t>( n );
-    h->task_counts    = a.take<uint32_t>( 64 );
-    h->error          = a.take<uint32_t>( 1 );
-    c.error           = h->error;
-    c.scene           = h->scene;
-    h->out.vcount     = a.take<uint32_t>( n );
-    h->out.ccount     = a.take<uint32_t>( n );
-    h->out.tile_sums  = a.take<uint32_t>( scanWords * 2 );
-    h->out.totals     = a.take<uint64_t>( 2 );
-    spec_carve( h->spec, a.take<char>( spec_bytes( n ) ), n );
-    c.walk_scratch    = a.take<uint32_t>( walk_scratch_bytes() / sizeof( uint32_t ) );
-    sort_scratch_carve( h->sort, sortBase, n, h->error );
-    if ( a.used > a.size )
+    if ( !carve( h, n ) )
     {
-        cudaFree( a.base );
+        cudaFree( h->arena.base );
         delete h;
         return fail( APO2_ERR_CUDA, "arena accounting" );
     }
@@ -940,6 +979,258 @@ apo2_status apo2_radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t 
     const cudaError_t err = cudaGetLastError();
     if ( err != cudaSuccess )
         return cuda_fail( err, "sort launch" );
+    return APO2_OK;
+}
+
+} // extern "C"
+
+// -----------------------------------------------------------------------------------------
+// Batched form: many independent diagrams of uneven size (thousands of small protein-like
+// sets). Each of `streams` workers owns a handle sized for the largest diagram, a stream and a
+// host thread; diagrams go to whichever worker is free, largest first, so small builds overlap
+// on the GPU instead of queueing behind one another. A handle is re-pointed into its own
+// arena for each diagram's size (carve), so nothing is allocated while the batch runs.
+// -----------------------------------------------------------------------------------------
+struct apo2_batch
+{
+    uint32_t     max_sites = 0;
+    apo2_options options {};
+    int          device = 0;
+    struct Worker
+    {
+        apo2_handle * h  = nullptr;
+        cudaStream_t  s  = nullptr;
+        cudaEvent_t   e0 = nullptr, e1 = nullptr;
+        uint64_t *    words = nullptr; // pinned: vertex total, closed total, error word
+    };
+    std::vector<Worker> workers;
+};
+
+namespace
+{
+    void destroy_batch( apo2_batch * b )
+    {
+        if ( !b )
+            return;
+        cudaSetDevice( b->device );
+        for ( auto & w : b->workers )
+        {
+            if ( w.s )
+                cudaStreamSynchronize( w.s );
+            if ( w.h )
+                apo2_destroy( w.h );
+            if ( w.e0 )
+                cudaEventDestroy( w.e0 );
+            if ( w.e1 )
+                cudaEventDestroy( w.e1 );
+            if ( w.s )
+                cudaStreamDestroy( w.s );
+            if ( w.words )
+                cudaFreeHost( w.words );
+        }
+        delete b;
+    }
+
+    // One diagram on one worker: upload, build, extract, counts (and the vertices when asked).
+    apo2_status batch_one( apo2_batch::Worker & w, const float * sites, uint32_t n, bool want_vertices,
+                           std::vector<double4> & pos, std::vector<uint4> & ids, uint64_t & count, float & ms )
+    {
+        apo2_handle * h = w.h;
+        if ( !carve( h, n ) )
+            return fail( APO2_ERR_CUDA, "arena accounting" );
+        h->built     = false;
+        h->extracted = false;
+        APO2_CUDA( cudaMemsetAsync( h->bounds_counter, 0, sizeof( uint32_t ), w.s ), "batch reset" );
+        APO2_CUDA( cudaEventRecord( w.e0, w.s ), "batch event" );
+        APO2_CUDA( cudaMemcpyAsync( h->input, sites, sizeof( float4 ) * n, cudaMemcpyHostToDevice, w.s ), "batch upload" );
+        apo2_status st = enqueue_build( h, w.s );
+        if ( st == APO2_OK )
+            st = enqueue_extract( h, w.s );
+        if ( st != APO2_OK )
+            return st;
+        APO2_CUDA( cudaEventRecord( w.e1, w.s ), "batch event" );
+        APO2_CUDA( cudaMemcpyAsync( w.words, h->out.totals, 2 * sizeof( uint64_t ), cudaMemcpyDeviceToHost, w.s ), "batch counts" );
+        APO2_CUDA( cudaMemcpyAsync( w.words + 2, h->error, sizeof( uint32_t ), cudaMemcpyDeviceToHost, w.s ), "batch counts" );
+        APO2_CUDA( cudaStreamSynchronize( w.s ), "batch build" );
+        const uint32_t flags = uint32_t( w.words[ 2 ] & 0xffffffffu );
+        if ( flags )
+            return fail( APO2_ERR_CAPACITY, "capacity flags " + std::to_string( flags ) );
+        count = w.words[ 0 ];
+        if ( count > h->out.vcap )
+            return fail( APO2_ERR_CAPACITY, "batch output capacity" );
+        if ( want_vertices && count )
+        {
+            pos.resize( count );
+            ids.resize( count );
+            APO2_CUDA( cudaMemcpyAsync( pos.data(), h->out.vpos, sizeof( double4 ) * count, cudaMemcpyDeviceToHost, w.s ), "batch output" );
+            APO2_CUDA( cudaMemcpyAsync( ids.data(), h->out.vids, sizeof( uint4 ) * count, cudaMemcpyDeviceToHost, w.s ), "batch output" );
+            APO2_CUDA( cudaStreamSynchronize( w.s ), "batch output" );
+        }
+        APO2_CUDA( cudaEventElapsedTime( &ms, w.e0, w.e1 ), "batch timing" );
+        return APO2_OK;
+    }
+} // namespace
+
+extern "C" {
+
+apo2_status apo2_batch_create( uint32_t max_sites, uint32_t streams, const apo2_options * options, apo2_batch ** out )
+{
+    if ( !out || max_sites < 2 || streams == 0 || streams > 64 )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_batch_create" );
+    if ( max_sites > ( 1u << 28 ) )
+        return fail( APO2_ERR_TOO_LARGE, "at most 2^28 sites" );
+    apo2_options      opt {};
+    const apo2_status ost = normalize_options( options, opt );
+    if ( ost != APO2_OK )
+        return ost;
+    opt.stage_timing = 0;
+    APO2_CUDA( cudaSetDevice( int( opt.device ) ), "cudaSetDevice" );
+    configure_cell_kernels();
+    configure_spec_kernels();
+    apo2_batch * b = new ( std::nothrow ) apo2_batch {};
+    if ( !b )
+        return fail( APO2_ERR_OUT_OF_MEMORY, "host allocation" );
+    b->max_sites = max_sites;
+    b->options   = opt;
+    b->device    = int( opt.device );
+    b->workers.resize( streams );
+    for ( auto & w : b->workers )
+    {
+        apo2_handle * h = new ( std::nothrow ) apo2_handle {};
+        if ( !h )
+        {
+            destroy_batch( b );
+            return fail( APO2_ERR_OUT_OF_MEMORY, "host allocation" );
+        }
+        w.h          = h;
+        h->options   = opt;
+        h->device    = b->device;
+        h->input_f64 = false;
+        h->arena.size = arena_bytes( max_sites, opt, false );
+        cudaError_t err = cudaMalloc( reinterpret_cast<void **>( &h->arena.base ), h->arena.size );
+        if ( err == cudaSuccess && !carve( h, max_sites ) )
+            err = cudaErrorMemoryAllocation;
+        if ( err == cudaSuccess )
+            err = cudaStreamCreateWithFlags( &w.s, cudaStreamNonBlocking );
+        if ( err == cudaSuccess )
+            err = cudaEventCreate( &w.e0 );
+        if ( err == cudaSuccess )
+            err = cudaEventCreate( &w.e1 );
+        if ( err == cudaSuccess )
+            err = cudaMallocHost( reinterpret_cast<void **>( &w.words ), 4 * sizeof( uint64_t ) );
+        if ( err != cudaSuccess )
+        {
+            destroy_batch( b );
+            return cuda_fail( err, "batch allocation" );
+        }
+        const apo2_status st = ensure_output_capacity( h, 8 * uint64_t( max_sites ) + 1024, uint64_t( max_sites ) / 16 + 1024 );
+        if ( st != APO2_OK )
+        {
+            destroy_batch( b );
+            return st;
+        }
+    }
+    *out = b;
+    return APO2_OK;
+}
+
+apo2_status apo2_batch_build( apo2_batch * b, const float * sites_xyzr, const uint64_t * site_offsets, uint32_t count,
+                              uint64_t * vertex_offsets, double ** positions, uint32_t ** ids, float * build_ms )
+{
+    if ( !b || !sites_xyzr || !site_offsets || !vertex_offsets || ( ( positions == nullptr ) != ( ids == nullptr ) ) )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_batch_build" );
+    for ( uint32_t d = 0; d < count; d++ )
+    {
+        if ( site_offsets[ d + 1 ] < site_offsets[ d ] + 2 )
+            return fail( APO2_ERR_INVALID_ARG, "every diagram needs at least 2 sites" );
+        if ( site_offsets[ d + 1 ] - site_offsets[ d ] > b->max_sites )
+            return fail( APO2_ERR_TOO_LARGE, "a diagram is larger than the batch's max_sites" );
+    }
+    const bool want = positions != nullptr;
+    // largest diagrams first, so the last ones to finish are small
+    std::vector<uint32_t> order( count );
+    for ( uint32_t d = 0; d < count; d++ )
+        order[ d ] = d;
+    std::stable_sort( order.begin(), order.end(), [ & ]( uint32_t x, uint32_t y ) {
+        return site_offsets[ x + 1 ] - site_offsets[ x ] > site_offsets[ y + 1 ] - site_offsets[ y ];
+    } );
+    std::vector<std::vector<double4>> pos( want ? count : 0 );
+    std::vector<std::vector<uint4>>   idv( want ? count : 0 );
+    std::vector<uint64_t>             counts( count, 0 );
+    std::vector<float>                times( count, 0.f );
+    std::atomic<uint32_t>             next { 0 };
+    std::atomic<int>                  failed { 0 };
+    std::mutex                        error_mutex;
+    apo2_status                       first_status = APO2_OK;
+    std::string                       first_error;
+    std::vector<double4>              no_pos;
+    std::vector<uint4>                no_ids;
+
+    auto run = [ & ]( apo2_batch::Worker & w ) {
+        cudaSetDevice( b->device );
+        while ( !failed.load() )
+        {
+            const uint32_t k = next.fetch_add( 1 );
+            if ( k >= count )
+                break;
+            const uint32_t d  = order[ k ];
+            const uint32_t n  = uint32_t( site_offsets[ d + 1 ] - site_offsets[ d ] );
+            std::vector<double4> & p = want ? pos[ d ] : no_pos;
+            std::vector<uint4> &   q = want ? idv[ d ] : no_ids;
+            const apo2_status st = batch_one( w, sites_xyzr + 4 * site_offsets[ d ], n, want, p, q, counts[ d ], times[ d ] );
+            if ( st != APO2_OK )
+            {
+                std::lock_guard<std::mutex> lock( error_mutex );
+                if ( !failed.exchange( 1 ) )
+                {
+                    first_status = st;
+                    first_error  = "diagram " + std::to_string( d ) + ": " + g_last_error;
+                }
+            }
+        }
+    };
+    std::vector<std::thread> threads;
+    for ( size_t t = 1; t < b->workers.size(); t++ )
+        threads.emplace_back( run, std::ref( b->workers[ t ] ) );
+    run( b->workers[ 0 ] );
+    for ( auto & t : threads )
+        t.join();
+    if ( failed.load() )
+        return fail( first_status, first_error );
+
+    vertex_offsets[ 0 ] = 0;
+    for ( uint32_t d = 0; d < count; d++ )
+        vertex_offsets[ d + 1 ] = vertex_offsets[ d ] + counts[ d ];
+    if ( build_ms )
+        for ( uint32_t d = 0; d < count; d++ )
+            build_ms[ d ] = times[ d ];
+    if ( want )
+    {
+        const uint64_t total = vertex_offsets[ count ];
+        double *       P     = static_cast<double *>( std::malloc( sizeof( double4 ) * std::max<uint64_t>( total, 1 ) ) );
+        uint32_t *     I     = static_cast<uint32_t *>( std::malloc( sizeof( uint4 ) * std::max<uint64_t>( total, 1 ) ) );
+        if ( !P || !I )
+        {
+            std::free( P );
+            std::free( I );
+            return fail( APO2_ERR_OUT_OF_MEMORY, "batch output (host)" );
+        }
+        for ( uint32_t d = 0; d < count; d++ )
+        {
+            if ( !counts[ d ] )
+                continue;
+            std::memcpy( P + 4 * vertex_offsets[ d ], pos[ d ].data(), sizeof( double4 ) * counts[ d ] );
+            std::memcpy( I + 4 * vertex_offsets[ d ], idv[ d ].data(), sizeof( uint4 ) * counts[ d ] );
+        }
+        *positions = P;
+        *ids       = I;
+    }
+    return APO2_OK;
+}
+
+apo2_status apo2_batch_destroy( apo2_batch * b )
+{
+    destroy_batch( b );
     return APO2_OK;
 }
 

@@ -163,6 +163,8 @@ namespace apo2
         uint32_t   sub_cap      = 0;
     };
     size_t spec_bytes( uint32_t n );
+    // grid sizes of the speculation kernels (once per process; call before concurrent builds)
+    void configure_spec_kernels();
     void   spec_carve( SpecBuffers & b, void * base, uint32_t n );
     void   launch_edge_validation_speculative( const CellContext & c, const uint32_t * tasks, const uint32_t * task_count,
                                                const SpecBuffers & b, cudaStream_t s );

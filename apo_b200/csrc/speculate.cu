@@ -697,19 +697,24 @@ namespace apo2
 
     static int g_spec_grid = 0, g_heavy_grid = 0;
 
+    void configure_spec_kernels()
+    {
+        if ( g_spec_grid != 0 )
+            return;
+        int dev = 0, sms = 148, per_sm = 0;
+        cudaGetDevice( &dev );
+        cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_edge_speculate, kSpecBlock, 0 );
+        const int spec = sms * std::max( 1, per_sm );
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_edge_heavy, kHeavyBlock, 0 );
+        g_heavy_grid = sms * std::max( 1, per_sm );
+        g_spec_grid  = spec;
+    }
+
     void launch_edge_validation_speculative( const CellContext & c, const uint32_t * tasks, const uint32_t * task_count,
                                              const SpecBuffers & b, cudaStream_t s )
     {
-        if ( g_spec_grid == 0 )
-        {
-            int dev = 0, sms = 148, per_sm = 0;
-            cudaGetDevice( &dev );
-            cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_edge_speculate, kSpecBlock, 0 );
-            g_spec_grid = sms * std::max( 1, per_sm );
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_edge_heavy, kHeavyBlock, 0 );
-            g_heavy_grid = sms * std::max( 1, per_sm );
-        }
+        configure_spec_kernels();
         const uint32_t nbr_blocks = std::max( 1u, std::min<uint32_t>( ( c.n + 3 ) / 4, 148 * 32 ) );
         APO2_LAUNCH( "k_neighbor_lists", s, k_neighbor_lists<<<nbr_blocks, kNbrBlock, 0, s>>>( c, tasks, task_count, b ) );
         scan_exclusive( b.item_count, c.n, b.scan_sums, b.item_total, s );

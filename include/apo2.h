@@ -219,6 +219,24 @@ apo2_status apo2_radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t 
  * first call on a device looks the array up and should come before any stream capture. */
 apo2_status apo2_radix_sort_pairs_static( uint64_t * keys, uint32_t * values, uint32_t n, void * stream );
 
+/* Batched form: many independent diagrams of uneven size in one call (the reference builds one
+ * diagram per AlgorithmGPU object; a caller with thousands of small site sets loops over it,
+ * app/benchmarks/benchmark.cu:9-22). `streams` workers, each with its own stream, host thread and
+ * device memory for `max_sites` sites, take the diagrams largest first, so small builds overlap
+ * on the GPU. All allocation happens in apo2_batch_create. */
+typedef struct apo2_batch apo2_batch;
+apo2_status apo2_batch_create( uint32_t max_sites, uint32_t streams, const apo2_options * options, apo2_batch ** out );
+
+/* Builds `count` diagrams. Diagram d is sites_xyzr[4*site_offsets[d] .. 4*site_offsets[d+1]) (host,
+ * float x, y, z, r; at least 2 and at most max_sites sites). On return vertex_offsets[0..count]
+ * holds the prefix sums of the per-diagram output vertex counts; when positions and ids are not
+ * NULL they receive malloc'd arrays (release with apo2_free) of all diagrams' vertices in diagram
+ * order, as apo2_get_vertices gives them (ids index the diagram's own sites). build_ms (optional,
+ * count floats) receives each diagram's device time from its upload to the end of its extraction. */
+apo2_status apo2_batch_build( apo2_batch * b, const float * sites_xyzr, const uint64_t * site_offsets, uint32_t count,
+                              uint64_t * vertex_offsets, double ** positions, uint32_t ** ids, float * build_ms );
+apo2_status apo2_batch_destroy( apo2_batch * b );
+
 /* Seeded protein-like site set (host): `chains` self-avoiding random-walk chains of
  * `atoms_per_chain` atoms (bond 1.53 A, bond angle 109.5 +/- 10 deg, uniform torsion, van der
  * Waals radii mix) in a cube of `density` atoms per A^3, written as float (x, y, z, r).

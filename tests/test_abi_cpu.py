@@ -58,6 +58,9 @@ def test_host_argument_checks_without_device(lib):
     assert lib.apo2_build(None, None, 1) == 1
     assert lib.apo2_create(None, 0, 1, 0, None, None) == 1
     assert lib.apo2_radix_sort_pairs_static(None, None, 0, None) == 1
+    assert lib.apo2_batch_create(1, 4, None, None) == 1
+    assert lib.apo2_batch_build(None, None, None, 0, None, None, None, None) == 1
+    assert lib.apo2_batch_destroy(None) == 0
     keys = ctypes.c_void_p(16)
     assert lib.apo2_radix_sort_pairs_static(keys, keys, (1 << 20) + 1, None) == 7  # APO2_ERR_TOO_LARGE
     assert lib.apo2_radix_sort_scratch_bytes(1 << 20) + 256 <= 256 + 12853760 + 4096
