@@ -356,6 +356,73 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def batch_sets(count: int, lo: int, hi: int, seed: int = 3):
+    """Protein-like site sets with sizes log-uniform in [lo, hi] (chains of 100 atoms at
+    0.01 atoms/A^3, one seed per set)."""
+    from apo_b200 import generators as g
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(np.int64)
+    return [g.protein_chains(max(1, int(s) // 100), 100, 0.01, seed=int(seed * 100003 + d)) for d, s in enumerate(sizes)]
+
+
+def run_batch(args, world, rank, local):
+    """Batched form: `--sets` protein-like sets of log-uniform size, one step = all of them
+    through apo2_batch_build. Timed on the host around a device-synchronised call (the work
+    spans several streams); per-diagram latencies are CUDA-event times."""
+    import torch
+
+    import apo_b200
+    torch.cuda.set_device(local)
+    sets = batch_sets(args.sets, 200, 50000)
+    total = sum(int(d.shape[0]) for d in sets)
+    batch = apo_b200.Batch(max(int(d.shape[0]) for d in sets), streams=args.streams, device=local)
+    for _ in range(args.warmup):
+        batch.build(sets, vertices=False)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    lat = []
+    for _ in range(args.steps):
+        _, counts, ms = batch.build(sets, vertices=False)
+        lat.append(ms)
+    torch.cuda.synchronize()
+    step = (time.perf_counter() - t0) / args.steps
+    value, ms_max = aggregate_rate(total, step * 1e3, world, "cuda")
+    lat = np.concatenate(lat)
+    # end to end: the vertices of every diagram downloaded too
+    t1 = time.perf_counter()
+    out, counts, _ = batch.build(sets, vertices=True)
+    e2e_s = time.perf_counter() - t1
+    vertices = int(counts.sum())
+    del out
+    # the same sets one diagram at a time through the single-diagram API (first 256 sets)
+    t2 = time.perf_counter()
+    loop_sites = 0
+    for d in sets[:256]:
+        a = apo_b200.AlgorithmGPU(d, device=local)
+        a.build_and_extract()
+        a.output_counts()
+        a.close()
+        loop_sites += int(d.shape[0])
+    loop_rate = loop_sites / (time.perf_counter() - t2)
+    batch.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"batched protein-like sets ({args.sets}, sizes log-uniform 200-50000)", "sites": total,
+                   "streams": args.streams, "vertices": vertices, "timing": "host clock around synchronised batch calls",
+                   "parallelism": f"replicas{world}"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "loop_of_single_builds": {"value": loop_rate, "unit": UNIT, "sets": min(256, len(sets))},
+        "e2e": {"value": total / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(16 * total),
+                "d2h_bytes_per_step": int(48 * vertices)},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -366,11 +433,15 @@ def main():
     ap.add_argument("--sites", type=int, default=None)
     ap.add_argument("--cpu-sample", type=int, default=100000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sets", type=int, default=4096, help="batch workload: number of site sets")
+    ap.add_argument("--streams", type=int, default=8, help="batch workload: concurrent workers")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "batch":
+            run_batch(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
