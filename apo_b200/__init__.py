@@ -93,6 +93,7 @@ SIGNATURES = {
     "apo2_radix_sort_pairs": (_I, [_P, _P, _U32, _P, _P]),
     "apo2_radix_sort_pairs_static": (_I, [_P, _P, _U32, _P]),
     "apo2_generate_chains": (_I, [_U32, _U32, ctypes.c_double, _U64, _P]),
+    "apo2_topology_json": (_I, [_P, _P, _U64, _P]),
     "apo2_batch_create": (_I, [_U32, _U32, _P, _P]),
     "apo2_batch_build": (_I, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "apo2_batch_destroy": (_I, [_P]),
@@ -232,6 +233,14 @@ class AlgorithmGPU:
         _check(self._lib.apo2_get_topology(self._h, qa.ctypes.data, q.value, ta.ctypes.data, t.value, ba.ctypes.data, b.value,
                                            ctypes.byref(q), ctypes.byref(t), ctypes.byref(b)))
         return Topology(quadrisectors=qa, trisectors=ta, bisectors=ba)
+
+    def topology_json(self) -> str:
+        """The topology as the reference's topology harness writes it (JSON text)."""
+        n = ctypes.c_uint64()
+        _check(self._lib.apo2_topology_json(self._h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        _check(self._lib.apo2_topology_json(self._h, buf, n.value + 1, ctypes.byref(n)))
+        return buf.value.decode()
 
     def cell(self, site: int) -> tuple[np.ndarray, np.ndarray]:
         """Per-cell store of one input site: vertices (j, k, l, type) and edges (j, k, count)."""

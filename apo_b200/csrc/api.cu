@@ -603,13 +603,14 @@ apo2_status apo2_get_closed_edges( apo2_handle * h, double * positions, uint32_t
     return copy_output( h, true, positions, ids, capacity, location, written );
 }
 
-apo2_status apo2_get_topology( apo2_handle * h, uint32_t * quad, uint64_t quad_cap, uint32_t * tri, uint64_t tri_cap,
-                               uint32_t * bi, uint64_t bi_cap, uint64_t * quad_count, uint64_t * tri_count, uint64_t * bi_count )
+} // extern "C"
+
+namespace
 {
-    if ( !h )
-        return fail( APO2_ERR_INVALID_ARG, "null handle" );
-    if ( !h->built )
-        return fail( APO2_ERR_NOT_BUILT, "no build yet" );
+    // Unique bisectors, trisectors and quadrisectors, per sorted cell with the cell's id
+    // smallest, mapped to original ids (algorithm.inl:1732-1821).
+    apo2_status topology_arrays( apo2_handle * h, std::vector<uint32_t> & q, std::vector<uint32_t> & t, std::vector<uint32_t> & b )
+    {
     APO2_CUDA( cudaDeviceSynchronize(), "topology" );
     const uint32_t n        = h->n;
     const auto     vnb      = download( h->cells.vertex_nb, n );
@@ -617,8 +618,6 @@ apo2_status apo2_get_topology( apo2_handle * h, uint32_t * quad, uint64_t quad_c
     const auto     vertices = download( h->cells.vertices, size_t( n ) * kMaxVertices );
     const auto     edges    = download( h->cells.edges, size_t( n ) * kMaxEdges );
     const auto     ix       = download( h->tree.indices, n );
-    std::vector<uint32_t> q, t, b;
-    // per sorted cell: unique tuples with the cell's id smallest (algorithm.inl:1732-1821)
     std::vector<std::pair<uint32_t, uint32_t>> bis;
     std::vector<std::tuple<uint32_t, uint32_t>> tris;
     std::vector<std::tuple<uint32_t, uint32_t, uint32_t>> quads;
@@ -656,6 +655,23 @@ apo2_status apo2_get_topology( apo2_handle * h, uint32_t * quad, uint64_t quad_c
         for ( auto & x : quads )
             q.insert( q.end(), { ix[ i ], ix[ std::get<0>( x ) ], ix[ std::get<1>( x ) ], ix[ std::get<2>( x ) ] } );
     }
+    return APO2_OK;
+    }
+} // namespace
+
+extern "C" {
+
+apo2_status apo2_get_topology( apo2_handle * h, uint32_t * quad, uint64_t quad_cap, uint32_t * tri, uint64_t tri_cap,
+                               uint32_t * bi, uint64_t bi_cap, uint64_t * quad_count, uint64_t * tri_count, uint64_t * bi_count )
+{
+    if ( !h )
+        return fail( APO2_ERR_INVALID_ARG, "null handle" );
+    if ( !h->built )
+        return fail( APO2_ERR_NOT_BUILT, "no build yet" );
+    std::vector<uint32_t> q, t, b;
+    const apo2_status     st = topology_arrays( h, q, t, b );
+    if ( st != APO2_OK )
+        return st;
     if ( quad_count )
         *quad_count = q.size() / 4;
     if ( tri_count )
@@ -670,6 +686,49 @@ apo2_status apo2_get_topology( apo2_handle * h, uint32_t * quad, uint64_t quad_c
         std::memcpy( tri, t.data(), t.size() * 4 );
     if ( bi )
         std::memcpy( bi, b.data(), b.size() * 4 );
+    return APO2_OK;
+}
+
+apo2_status apo2_topology_json( apo2_handle * h, char * json, uint64_t capacity, uint64_t * length )
+{
+    if ( !h || !length )
+        return fail( APO2_ERR_INVALID_ARG, "null argument" );
+    if ( !h->built )
+        return fail( APO2_ERR_NOT_BUILT, "no build yet" );
+    std::vector<uint32_t> q, t, b;
+    const apo2_status     st = topology_arrays( h, q, t, b );
+    if ( st != APO2_OK )
+        return st;
+    // the layout of the reference's topology writer (app/topology/topology.cpp:11-57)
+    std::string out = "{\n\t\"bisectors\": [\n";
+    char        line[ 96 ];
+    const size_t nb = b.size() / 2, nt = t.size() / 3, nq = q.size() / 4;
+    for ( size_t x = 0; x < nb; x++ )
+    {
+        std::snprintf( line, sizeof( line ), "\t\t[ %u, %u ]%s\n", b[ 2 * x ], b[ 2 * x + 1 ], x + 1 == nb ? "" : "," );
+        out += line;
+    }
+    out += "\t],\n\t\"trisectors\": [\n";
+    for ( size_t x = 0; x < nt; x++ )
+    {
+        std::snprintf( line, sizeof( line ), "\t\t[ %u, %u, %u ]%s\n", t[ 3 * x ], t[ 3 * x + 1 ], t[ 3 * x + 2 ], x + 1 == nt ? "" : "," );
+        out += line;
+    }
+    out += "\t],\n\t\"quadrisectors\": [\n";
+    for ( size_t x = 0; x < nq; x++ )
+    {
+        std::snprintf( line, sizeof( line ), "\t\t[ %u, %u, %u, %u ]%s\n", q[ 4 * x ], q[ 4 * x + 1 ], q[ 4 * x + 2 ], q[ 4 * x + 3 ],
+                       x + 1 == nq ? "" : "," );
+        out += line;
+    }
+    out += "\t]\n}\n";
+    *length = out.size();
+    if ( json )
+    {
+        if ( capacity < out.size() + 1 )
+            return fail( APO2_ERR_INVALID_ARG, "json capacity too small" );
+        std::memcpy( json, out.c_str(), out.size() + 1 );
+    }
     return APO2_OK;
 }
 

@@ -161,6 +161,12 @@ apo2_status apo2_get_topology( apo2_handle * h, uint32_t * quadrisectors, uint64
                                uint64_t bi_capacity, uint64_t * quad_count, uint64_t * tri_count,
                                uint64_t * bi_count );
 
+/* The topology as the JSON text the reference's topology harness writes
+ * (app/topology/topology.cpp:11-57, same layout and order: "bisectors", "trisectors",
+ * "quadrisectors" lists of id tuples). *length receives the text's size without the NUL; with
+ * json == NULL only the size is computed, otherwise capacity must hold length + 1 bytes. */
+apo2_status apo2_topology_json( apo2_handle * h, char * json, uint64_t capacity, uint64_t * length );
+
 /* Per-cell store of one site (given by original id): its vertices as (j, k, l, type) and
  * edges as (j, k, vertex count or 0xffffffff for a closed trisector), ids original. */
 apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, uint32_t vertex_capacity,

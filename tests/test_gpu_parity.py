@@ -241,3 +241,18 @@ def test_edge_search_modes_agree(apo, case):
         algo.close()
     for name in stores[0]:
         assert np.array_equal(stores[0][name], stores[1][name]), name
+
+
+def test_topology_json_matches_topology(apo):
+    """The JSON writer gives the reference harness's layout with the same tuples as toTopology."""
+    import json
+    golden = H.load_golden("prec1")
+    algo = apo.AlgorithmGPU(H.sites_for("prec1"))
+    algo.build()
+    text = algo.topology_json()
+    assert text.startswith('{\n\t"bisectors": [\n\t\t[ ') and text.endswith("\t]\n}\n")
+    data = json.loads(text)
+    assert np.array_equal(np.asarray(data["bisectors"], np.uint32).reshape(-1), golden["topo_bi"])
+    assert np.array_equal(np.asarray(data["trisectors"], np.uint32).reshape(-1), golden["topo_tri"])
+    assert np.array_equal(np.asarray(data["quadrisectors"], np.uint32).reshape(-1), golden["topo_quad"])
+    algo.close()
