@@ -94,6 +94,7 @@ SIGNATURES = {
     "apo2_radix_sort_pairs_static": (_I, [_P, _P, _U32, _P]),
     "apo2_generate_chains": (_I, [_U32, _U32, ctypes.c_double, _U64, _P]),
     "apo2_topology_json": (_I, [_P, _P, _U64, _P]),
+    "apo2_certify": (_I, [_P, _P, _P, _U64, _U32, _I, _P, _P]),
     "apo2_batch_create": (_I, [_U32, _U32, _P, _P]),
     "apo2_batch_build": (_I, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "apo2_batch_destroy": (_I, [_P]),
@@ -233,6 +234,22 @@ class AlgorithmGPU:
         _check(self._lib.apo2_get_topology(self._h, qa.ctypes.data, q.value, ta.ctypes.data, t.value, ba.ctypes.data, b.value,
                                            ctypes.byref(q), ctypes.byref(t), ctypes.byref(b)))
         return Topology(quadrisectors=qa, trisectors=ta, bisectors=ba)
+
+    def certify(self, positions=None, ids=None, arity: int = 4):
+        """Interval certificate (the reference's precision check) of the handle's output
+        (positions/ids None) or of given points: returns (bad count, per-point flags)."""
+        bad = ctypes.c_uint64()
+        if positions is None:
+            count = self.output_counts()[0 if arity == 4 else 1]
+            flags = np.zeros(max(count, 1), dtype=np.uint8)
+            _check(self._lib.apo2_certify(self._h, None, None, 0, arity, APO2_HOST, flags.ctypes.data, ctypes.byref(bad)))
+            return bad.value, flags[:count]
+        p = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 4))
+        i = np.ascontiguousarray(np.asarray(ids, dtype=np.uint32).reshape(-1, 4))
+        flags = np.zeros(max(p.shape[0], 1), dtype=np.uint8)
+        _check(self._lib.apo2_certify(self._h, p.ctypes.data, i.ctypes.data, p.shape[0], arity, APO2_HOST,
+                                      flags.ctypes.data, ctypes.byref(bad)))
+        return bad.value, flags[:p.shape[0]]
 
     def topology_json(self) -> str:
         """The topology as the reference's topology harness writes it (JSON text)."""

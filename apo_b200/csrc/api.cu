@@ -732,6 +732,81 @@ apo2_status apo2_topology_json( apo2_handle * h, char * json, uint64_t capacity,
     return APO2_OK;
 }
 
+apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint32_t * ids, uint64_t count, uint32_t arity,
+                          apo2_location location, uint8_t * flags, uint64_t * bad )
+{
+    if ( !h || !bad || ( arity != 3 && arity != 4 ) || ( ( positions == nullptr ) != ( ids == nullptr ) )
+         || ( location != APO2_HOST && location != APO2_DEVICE ) )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_certify" );
+    if ( !h->built )
+        return fail( APO2_ERR_NOT_BUILT, "no build yet" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    const double4 * P = nullptr;
+    const uint4 *   I = nullptr;
+    void *          scratch = nullptr;
+    if ( !positions )
+    {
+        // the handle's own extracted output
+        apo2_status st = settle_output( h, 0 );
+        if ( st != APO2_OK )
+            return st;
+        uint64_t totals[ 2 ];
+        APO2_CUDA( cudaMemcpy( totals, h->out.totals, sizeof( totals ), cudaMemcpyDeviceToHost ), "output totals" );
+        count = arity == 4 ? totals[ 0 ] : totals[ 1 ];
+        P     = arity == 4 ? h->out.vpos : h->out.cpos;
+        I     = arity == 4 ? h->out.vids : h->out.cids;
+    }
+    const size_t flag_bytes = align256( std::max<uint64_t>( count, 1 ) );
+    const size_t in_bytes   = positions && location == APO2_HOST ? align256( sizeof( double4 ) * count ) + align256( sizeof( uint4 ) * count ) : 0;
+    APO2_CUDA( cudaMalloc( &scratch, 256 + flag_bytes + in_bytes ), "certify scratch" );
+    char *               base  = static_cast<char *>( scratch );
+    unsigned long long * dbad  = reinterpret_cast<unsigned long long *>( base );
+    uint8_t *            dflag = reinterpret_cast<uint8_t *>( base + 256 );
+    if ( positions )
+    {
+        if ( location == APO2_HOST )
+        {
+            double4 * dp = reinterpret_cast<double4 *>( base + 256 + flag_bytes );
+            uint4 *   di = reinterpret_cast<uint4 *>( base + 256 + flag_bytes + align256( sizeof( double4 ) * count ) );
+            cudaMemcpy( dp, positions, sizeof( double4 ) * count, cudaMemcpyHostToDevice );
+            cudaMemcpy( di, ids, sizeof( uint4 ) * count, cudaMemcpyHostToDevice );
+            P = dp;
+            I = di;
+        }
+        else
+        {
+            P = reinterpret_cast<const double4 *>( positions );
+            I = reinterpret_cast<const uint4 *>( ids );
+        }
+    }
+    cudaMemset( dbad, 0, sizeof( unsigned long long ) );
+    cudaMemset( h->error, 0, sizeof( uint32_t ) );
+    Scene scene;
+    cudaMemcpy( &scene, h->scene, sizeof( Scene ), cudaMemcpyDeviceToHost );
+    if ( count )
+    {
+        ObserveScope observe( h );
+        launch_certify( h->input_d4, h->tree.sites, h->tree.indices, h->tree.nodes, h->n, P, I, arity, count, float( scene.rmax ),
+                        dflag, dbad, h->error, 0 );
+    }
+    unsigned long long nbad = 0;
+    uint32_t           err  = 0;
+    cudaError_t        e    = cudaDeviceSynchronize();
+    if ( e == cudaSuccess )
+        e = cudaMemcpy( &nbad, dbad, sizeof( nbad ), cudaMemcpyDeviceToHost );
+    if ( e == cudaSuccess )
+        e = cudaMemcpy( &err, h->error, sizeof( err ), cudaMemcpyDeviceToHost );
+    if ( e == cudaSuccess && flags && count )
+        e = cudaMemcpy( flags, dflag, count, cudaMemcpyDeviceToHost );
+    cudaFree( scratch );
+    if ( e != cudaSuccess )
+        return cuda_fail( e, "certify" );
+    if ( err )
+        return fail( APO2_ERR_CAPACITY, "certify walk flags " + std::to_string( err ) );
+    *bad = nbad;
+    return APO2_OK;
+}
+
 apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, uint32_t vcap, uint32_t * vcount,
                            uint32_t * edges, uint32_t ecap, uint32_t * ecount )
 {

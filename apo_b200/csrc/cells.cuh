@@ -163,6 +163,11 @@ namespace apo2
         uint32_t   sub_cap      = 0;
     };
     size_t spec_bytes( uint32_t n );
+    // interval certificate of output points (certify.cu): flags (optional) and a count of the
+    // points some other site is certainly closer to than their defining sites
+    void launch_certify( const double4 * by_id, const double4 * sorted, const uint32_t * indices, const WideNode * nodes,
+                         uint32_t n, const double4 * points, const uint4 * ids, uint32_t arity, uint64_t count, float rmax,
+                         uint8_t * flags, unsigned long long * bad, uint32_t * error, cudaStream_t s );
     // grid sizes of the speculation kernels (once per process; call before concurrent builds)
     void configure_spec_kernels();
     void   spec_carve( SpecBuffers & b, void * base, uint32_t n );

@@ -167,6 +167,17 @@ apo2_status apo2_get_topology( apo2_handle * h, uint32_t * quadrisectors, uint64
  * json == NULL only the size is computed, otherwise capacity must hold length + 1 bytes. */
 apo2_status apo2_topology_json( apo2_handle * h, char * json, uint64_t capacity, uint64_t * length );
 
+/* Interval certificate of output points, as the reference's precision check
+ * (app/precision/precision.cpp:14-163): every weighted distance |c - p| - r is an outward-rounded
+ * interval, and a point is bad when a site other than its own is certainly closer than the
+ * largest of its own sites' distances. arity 4 checks vertices (ids i, j, k, l), 3 closed
+ * edges (ids i, j, k). positions/ids: double[4*count] / uint32[4*count] (original site ids) on
+ * the host or the device; both NULL certifies the handle's last extracted output (count is
+ * then taken from it). flags (optional, host, count bytes) receives 1 for each bad point. The
+ * search walks the handle's BVH instead of all sites. */
+apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint32_t * ids, uint64_t count, uint32_t arity,
+                          apo2_location location, uint8_t * flags, uint64_t * bad );
+
 /* Per-cell store of one site (given by original id): its vertices as (j, k, l, type) and
  * edges as (j, k, vertex count or 0xffffffff for a closed trisector), ids original. */
 apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, uint32_t vertex_capacity,

@@ -58,6 +58,8 @@ def test_host_argument_checks_without_device(lib):
     assert lib.apo2_build(None, None, 1) == 1
     assert lib.apo2_create(None, 0, 1, 0, None, None) == 1
     assert lib.apo2_radix_sort_pairs_static(None, None, 0, None) == 1
+    assert lib.apo2_certify(None, None, None, 0, 4, 0, None, None) == 1
+    assert lib.apo2_topology_json(None, None, 0, None) == 1
     assert lib.apo2_batch_create(1, 4, None, None) == 1
     assert lib.apo2_batch_build(None, None, None, 0, None, None, None, None) == 1
     assert lib.apo2_batch_destroy(None) == 0
