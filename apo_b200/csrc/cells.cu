@@ -93,6 +93,37 @@ namespace apo2
         return true;
     }
 
+#ifndef APO2_LANE_CLEAR_EDGES
+#define APO2_LANE_CLEAR_EDGES 32
+#endif
+    // cells with at most this many edges check new roots lane by lane in update_cell
+    constexpr uint32_t kLaneClearEdges = APO2_LANE_CLEAR_EDGES;
+
+    // Lane-local forms of is_known / edges_clear (same predicates, one lane scanning all edges).
+    __device__ __forceinline__ bool known_by_lane( const WarpCell & w, uint32_t id )
+    {
+        for ( uint32_t e = 0; e < w.en; e++ )
+        {
+            const uint4 r = w.e[ e ];
+            if ( r.x == id || r.y == id )
+                return true;
+        }
+        return false;
+    }
+    __device__ __forceinline__ bool clear_by_lane( const CellContext & c, const WarpCell & w, double4 sphere, uint32_t skip1,
+                                                   uint32_t skip2 )
+    {
+        for ( uint32_t e = 0; e < w.en; e++ )
+        {
+            const uint4 r = w.e[ e ];
+            if ( r.x != skip1 && r.x != skip2 && intersects( site( c, r.x ), sphere ) )
+                return false;
+            if ( r.y != skip1 && r.y != skip2 && intersects( site( c, r.y ), sphere ) )
+                return false;
+        }
+        return true;
+    }
+
     // Is `id` already a neighbour of the cell (one of its edges' sites)? Warp-collective.
     __device__ __forceinline__ bool is_known( const WarpCell & w, uint32_t id )
     {
@@ -277,22 +308,38 @@ namespace apo2
                     w.e[ e ].z = 0;
             }
 
+            // The emptiness predicate of every root (topology_update.inl:577-590): on a small
+            // cell each lane checks its own roots against every edge site; on a large one the
+            // whole warp checks one root at a time, 32 edges per step.
             uint32_t valid = mask;
-            uint32_t hm    = __ballot_sync( kFull, has );
-            while ( hm )
+            if ( baseE <= kLaneClearEdges )
             {
-                const uint32_t t = highest( hm );
-                hm &= ~( 1u << t );
-                uint32_t       tm = __shfl_sync( kFull, mask, t );
-                const uint32_t tk = __shfl_sync( kFull, k, t ), tl = __shfl_sync( kFull, l, t );
-                while ( tm )
+                if ( has )
                 {
-                    const uint32_t nv = __ffs( tm ) - 1;
-                    tm &= ~( 1u << nv );
-                    const double4 cand = shfl4( nv ? q1 : q0, t );
-                    const bool    ok   = edges_clear( c, w, cand, tk, tl );
-                    if ( lane == t && !ok )
-                        valid &= ~( 1u << nv );
+                    if ( ( mask & 1u ) && !clear_by_lane( c, w, q0, k, l ) )
+                        valid &= ~1u;
+                    if ( ( mask & 2u ) && !clear_by_lane( c, w, q1, k, l ) )
+                        valid &= ~2u;
+                }
+            }
+            else
+            {
+                uint32_t hm = __ballot_sync( kFull, has );
+                while ( hm )
+                {
+                    const uint32_t t = highest( hm );
+                    hm &= ~( 1u << t );
+                    uint32_t       tm = __shfl_sync( kFull, mask, t );
+                    const uint32_t tk = __shfl_sync( kFull, k, t ), tl = __shfl_sync( kFull, l, t );
+                    while ( tm )
+                    {
+                        const uint32_t nv = __ffs( tm ) - 1;
+                        tm &= ~( 1u << nv );
+                        const double4 cand = shfl4( nv ? q1 : q0, t );
+                        const bool    ok   = edges_clear( c, w, cand, tk, tl );
+                        if ( lane == t && !ok )
+                            valid &= ~( 1u << nv );
+                    }
                 }
             }
 
@@ -1057,31 +1104,6 @@ namespace apo2
     {
         return make_float4( __shfl_sync( kFull, v.x, src ), __shfl_sync( kFull, v.y, src ), __shfl_sync( kFull, v.z, src ),
                             __shfl_sync( kFull, v.w, src ) );
-    }
-
-    // Lane-local forms of is_known / edges_clear (same predicates, one lane scanning all edges).
-    __device__ __forceinline__ bool known_by_lane( const WarpCell & w, uint32_t id )
-    {
-        for ( uint32_t e = 0; e < w.en; e++ )
-        {
-            const uint4 r = w.e[ e ];
-            if ( r.x == id || r.y == id )
-                return true;
-        }
-        return false;
-    }
-    __device__ __forceinline__ bool clear_by_lane( const CellContext & c, const WarpCell & w, double4 sphere, uint32_t skip1,
-                                                   uint32_t skip2 )
-    {
-        for ( uint32_t e = 0; e < w.en; e++ )
-        {
-            const uint4 r = w.e[ e ];
-            if ( r.x != skip1 && r.x != skip2 && intersects( site( c, r.x ), sphere ) )
-                return false;
-            if ( r.y != skip1 && r.y != skip2 && intersects( site( c, r.y ), sphere ) )
-                return false;
-        }
-        return true;
     }
 
     // The rest of a long edge search, walked by the whole warp in the lane walk's order.
