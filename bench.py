@@ -46,7 +46,8 @@ C_TEST = 11
 # DRAM bytes (read + write) per site of one build, by kernel, from one ncu capture of the
 # protein-like packing at 100,000 sites (profiles/top_kernels_protein100k.md), scaled by the
 # sites processed.
-TRAFFIC_BYTES_PER_SITE = {"k_vertex_validation": 1871.8, "k_edge_speculate": 1527.0, "k_cells": 304.0}
+TRAFFIC_BYTES_PER_SITE = {"k_vertex_validation": 1839.3, "k_edge_speculate": 1536.5, "k_cells": 316.6,
+                          "k_bisector_validation": 1054.6}
 
 
 def measure_fp64_peak(device) -> float:
