@@ -343,7 +343,7 @@ namespace
         total += align256( 4 * size_t( n ) ) + align256( 4 * 64 ) + align256( 4 );
         total += align256( 4 * size_t( n ) ) * 2 + align256( 4 * scanWords * 2 ) + align256( 16 );
         total += align256( spec_bytes( n ) );
-        total += align256( walk_scratch_bytes() );
+        total += align256( walk_scratch_bytes() ) + align256( 4 );
         return total;
     }
 
@@ -402,6 +402,7 @@ namespace
         h->out.totals     = a.take<uint64_t>( 2 );
         spec_carve( h->spec, a.take<char>( spec_bytes( n ) ), n );
         c.walk_scratch    = a.take<uint32_t>( walk_scratch_bytes() / sizeof( uint32_t ) );
+        c.work_counter    = a.take<uint32_t>( 1 );
         sort_scratch_carve( h->sort, sortBase, n, h->error );
         return a.used <= a.size;
     }

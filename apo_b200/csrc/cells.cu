@@ -846,8 +846,17 @@ namespace apo2
         const uint32_t nwarp = gridDim.x * ( kCellBlock / 32 );
         WarpCell       w     = carve( smem, warp, 0 );
         uint32_t       err   = 0;
-        for ( uint32_t i = gwarp; i < c.n; i += nwarp )
+        // cells are taken one at a time from a shared counter (uneven cells, see bisector pass)
+        ( void ) gwarp;
+        ( void ) nwarp;
+        while ( true )
         {
+            uint32_t i = 0;
+            if ( lane_id() == 0 )
+                i = atomicAdd( c.work_counter, 1u );
+            i = __shfl_sync( kFull, i, 0 );
+            if ( i >= c.n )
+                break;
             if ( mode == kCellsInitOnly )
             {
                 initial_cell( c, w, c.sites[ i ] );
@@ -916,8 +925,17 @@ namespace apo2
         const uint32_t count = *task_count;
         const uint32_t n     = c.n;
         const float    rmax  = float( c.scene->rmax );
-        for ( uint32_t t = gwarp; t < count; t += nwarp )
+        // tasks are taken one at a time from a shared counter (uneven cells, see bisector pass)
+        ( void ) gwarp;
+        ( void ) nwarp;
+        while ( true )
         {
+            uint32_t t = 0;
+            if ( lane == 0 )
+                t = atomicAdd( c.work_counter, 1u );
+            t = __shfl_sync( kFull, t, 0 );
+            if ( t >= count )
+                break;
             const uint32_t i      = tasks[ t ];
             const uint8_t  status = c.status[ i ];
             if ( status == kFullyValidated || status == kBuried )
@@ -1239,8 +1257,16 @@ namespace apo2
         const uint32_t n     = c.n;
         uint32_t *     frontier = c.walk_scratch + size_t( gwarp ) * kWalkScratchWords;
         uint32_t *     saved    = frontier + kCoopCap + lane * ( kStack + 1 );
-        for ( uint32_t t = gwarp; t < count; t += nwarp )
+        // tasks are taken one at a time from a shared counter; `gwarp` only names the scratch
+        ( void ) nwarp;
+        while ( true )
         {
+            uint32_t t = 0;
+            if ( lane == 0 )
+                t = atomicAdd( c.work_counter, 1u );
+            t = __shfl_sync( kFull, t, 0 );
+            if ( t >= count )
+                break;
             const uint32_t i      = tasks[ t ];
             const uint8_t  status = c.status[ i ];
             if ( status == kFullyValidated || status == kBuried )
@@ -1558,19 +1584,25 @@ namespace apo2
     // -----------------------------------------------------------------------------------
     // Bisector validation (algorithm.inl:859-1233)
     // -----------------------------------------------------------------------------------
-    __global__ void __launch_bounds__( kCellBlock, 3 ) k_bisector_validation( CellContext c )
+    // Cells are taken one at a time from a shared counter: their costs are uneven (a few hold
+    // long searches), and a fixed share per warp left most warps idle at the end.
+    __global__ void __launch_bounds__( kCellBlock, 3 ) k_bisector_validation( CellContext c, uint32_t * __restrict__ next )
     {
         extern __shared__ __align__( 16 ) unsigned char smem[];
         const uint32_t warp  = threadIdx.x >> 5;
-        const uint32_t gwarp = blockIdx.x * ( kCellBlock / 32 ) + warp;
-        const uint32_t nwarp = gridDim.x * ( kCellBlock / 32 );
         const uint32_t lane  = lane_id();
         WarpCell       w     = carve( smem, warp, kBisectorBytes );
         uint32_t *     bis   = reinterpret_cast<uint32_t *>( reinterpret_cast<unsigned char *>( w.e ) + sizeof( uint4 ) * kEdgeSlots );
         uint32_t       err   = 0;
         const uint32_t n     = c.n;
-        for ( uint32_t i = gwarp; i < n; i += nwarp )
+        while ( true )
         {
+            uint32_t i = 0;
+            if ( lane == 0 )
+                i = atomicAdd( next, 1u );
+            i = __shfl_sync( kFull, i, 0 );
+            if ( i >= n )
+                break;
             if ( c.status[ i ] == kBuried )
                 continue;
             const float   known = c.known_radii[ i ];
@@ -2077,6 +2109,7 @@ namespace apo2
 
     void launch_cells( const CellContext & c, uint32_t mode, cudaStream_t s )
     {
+        cudaMemsetAsync( c.work_counter, 0, sizeof( uint32_t ), s );
         APO2_LAUNCH( "k_cells", s, k_cells<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, mode ) );
     }
 
@@ -2088,18 +2121,21 @@ namespace apo2
 
     void launch_vertex_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s )
     {
+        cudaMemsetAsync( c.work_counter, 0, sizeof( uint32_t ), s );
         APO2_LAUNCH( "k_vertex_validation", s, k_vertex_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, tasks, count ) );
     }
 
     void launch_edge_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s,
                                  SearchProof proof )
     {
+        cudaMemsetAsync( c.work_counter, 0, sizeof( uint32_t ), s );
         APO2_LAUNCH( "k_edge_validation", s, k_edge_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, tasks, count, proof ) );
     }
 
     void launch_bisector_validation( const CellContext & c, cudaStream_t s )
     {
-        APO2_LAUNCH( "k_bisector_validation", s, k_bisector_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( true ), s>>>( c ) );
+        cudaMemsetAsync( c.work_counter, 0, sizeof( uint32_t ), s );
+        APO2_LAUNCH( "k_bisector_validation", s, k_bisector_validation<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( true ), s>>>( c, c.work_counter ) );
     }
 
     void launch_output( const CellContext & c, const OutputBuffers & o, cudaStream_t s )

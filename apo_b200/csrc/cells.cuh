@@ -40,6 +40,7 @@ namespace apo2
         uint32_t *       error       = nullptr;
         const Scene *    scene       = nullptr; // bounds and radius range of the sites
         uint32_t *       walk_scratch = nullptr; // kWalkScratchWords per warp of the exact edge pass
+        uint32_t *       work_counter = nullptr; // next cell of the dynamically scheduled passes
     };
 
     // Exact edge validation: a lane walks its edge's search alone for kLaneWalk steps; a
