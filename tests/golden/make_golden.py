@@ -49,6 +49,10 @@ CASES = {
     "protein20k": ("protein_chains(40, 500, 0.01, seed=3)", False),
     "latticeA20": ("lattice(20, 'A', seed=4)", False),
     "latticeB20": ("lattice(20, 'B', seed=5)", False),
+    # larger clouds: the edge-parallel search, its long-search paths and the exact pass at scale
+    "uni100k": ("uniform_cloud(100000, 215.44, 1.5, 0.5)", False),
+    "logn50k": ("lognormal_cloud(50000, 400.0 * (0.01 ** (1 / 3)), seed=9)", False),
+    "protein100k": ("protein_chains(200, 500, 0.01, seed=1)", False),
 }
 
 
