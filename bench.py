@@ -259,6 +259,10 @@ def run_ours(args, world, rank, local):
     ms = start.elapsed_time(stop) / args.steps
     value, ms_max = aggregate_rate(n, ms, world, device)
     err = algo.stats()["error_flags"]
+    # interval certificate of every output vertex (the reference's precision check, on the GPU)
+    t_c = time.perf_counter()
+    bad_vertices, _ = algo.certify()
+    certificate = {"vertices": int(vcount), "bad": int(bad_vertices), "seconds": round(time.perf_counter() - t_c, 3)}
 
     # --- per-kernel times of one more build (events around every launch) ---
     prof_algo = apo_b200.AlgorithmGPU(sites, device=local, stage_timing=True)
@@ -352,6 +356,7 @@ def run_ours(args, world, rank, local):
                        vertices=int(vcount), closed_edges=int(ccount), error_flags=int(err),
                        validation_rounds=int(stats["validation_rounds"])),
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(), "gpu_launches": launches * args.steps,
+        "certificate": certificate,
         "kernel_ms": {k: round(v[1], 3) for k, v in sorted(kernels.items(), key=lambda kv: -kv[1][1])[:8]},
     }
     print(json.dumps(line), flush=True)
