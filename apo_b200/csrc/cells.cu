@@ -1134,6 +1134,87 @@ namespace apo2
     // is it or a leaf under one of the q nodes before it: everything after it is dropped and
     // the walk continues over those. `saved` holds the suspended lane's position (its current
     // node, then its stack from the top), `count` entries, earliest first.
+    // One frontier node of the ordered walk: an internal node gives its entered children in walk
+    // order (kids, first, second), a leaf whether it contributes.
+    __device__ __forceinline__ void ordered_step( const CellContext & c, const WarpCell & w, uint32_t i, double4 si,
+                                                  const EdgeWalk & p, uint32_t node, uint32_t & kids, uint32_t & first,
+                                                  uint32_t & second, bool & contrib, uint32_t & j )
+    {
+        const uint32_t n = c.n;
+        kids             = 0;
+        contrib          = false;
+        j                = kNone;
+        if ( node < n - 1 )
+        {
+            Box      lb, rb;
+            uint32_t lc, rc;
+            load_node( c.nodes, node, lb, rb, lc, rc );
+            const float3   closeL = lb.closest( p.bsph ), closeR = rb.closest( p.bsph );
+            const float    dL = lb.distance( p.bsph ), dR = rb.distance( p.bsph );
+            const bool     leftClosest = dL < dR;
+            const float    minFar = leftClosest ? dR : dL, minClose = leftClosest ? dL : dR;
+            const float3   farPoint = leftClosest ? closeR : closeL, closePoint = leftClosest ? closeL : closeR;
+            const uint32_t farChild = leftClosest ? rc : lc, closeChild = leftClosest ? lc : rc;
+            bool           exploreFar = minFar < 0.f;
+            if ( p.hyperbola && exploreFar )
+                exploreFar = fdot( p.n1, farPoint - p.pp1 ) < 0.f && fdot( p.n2, farPoint - p.pp2 ) < 0.f;
+            bool exploreClose = minClose < 0.f;
+            if ( p.hyperbola && exploreClose )
+                exploreClose = fdot( p.n1, closePoint - p.pp1 ) < 0.f && fdot( p.n2, closePoint - p.pp2 ) < 0.f;
+            exploreFar   = exploreFar && ( leftClosest ? rb : lb ).distance( p.reach ) < 0.f;
+            exploreClose = exploreClose && ( leftClosest ? lb : rb ).distance( p.reach ) < 0.f;
+            if ( exploreClose )
+            {
+                first = closeChild;
+                kids  = 1;
+                if ( exploreFar )
+                {
+                    second = farChild;
+                    kids   = 2;
+                }
+            }
+            else if ( exploreFar )
+            {
+                first = farChild;
+                kids  = 1;
+            }
+        }
+        else if ( node < 2 * n - 1 )
+        {
+            j        = node - ( n - 1 );
+            bool can = j != i && j != p.k && j != p.l && c.status[ j ] != kBuried;
+            double4 sj = make_double4( 0, 0, 0, 0 );
+            if ( can )
+            {
+                sj              = c.sites[ j ];
+                const float4 fj = to_float( sj );
+                can             = intersects( fj, p.bsph ) && flength( f3( fj ) - f3( p.reach ) ) <= p.reach.w;
+                if ( p.hyperbola )
+                    can = can && double( fdot( p.n1, f3( fj ) - p.pp1 ) ) < -sj.w
+                          && double( fdot( p.n2, f3( fj ) - p.pp2 ) ) < -sj.w;
+            }
+            if ( can )
+                can = !known_by_lane( w, j );
+            if ( can )
+            {
+                double4 x0 = make_double4( 0, 0, 0, 0 ), x1 = make_double4( 0, 0, 0, 0 );
+                const uint32_t mask = quadrisector( si, sj, p.sk, p.sl, x0, x1 );
+                contrib = mask == 3 && ( clear_by_lane( c, w, x0, p.k, p.l ) || clear_by_lane( c, w, x1, p.k, p.l ) );
+            }
+        }
+    }
+
+    // The rest of a long edge search, walked by the whole warp in the lane walk's order.
+    // The walk has no running bound: which children of a node are entered, and in which order
+    // (closer first), depends on the node alone, so its leaves come in one fixed order and the
+    // answer is the first contributing leaf of that order. The frontier (nodes not yet expanded,
+    // in that order) is a stack in `frontier`, its earliest node on top. Each step expands the
+    // kCoopWidth x 32 earliest nodes at once (position r * 32 + lane for a lane's r-th node, so
+    // each lane's loads overlap): an internal node is replaced by its entered children, a leaf
+    // is tested. When the earliest contributing leaf of a step sits at position q, the answer
+    // is it or a leaf under one of the q nodes before it: everything after it is dropped and
+    // the walk continues over those. `saved` holds the suspended lane's position (its current
+    // node, then its stack from the top), `count` entries, earliest first.
     __device__ uint32_t ordered_edge_walk( const CellContext & c, const WarpCell & w, uint32_t i, double4 si, const EdgeWalk & p,
                                            uint32_t * frontier, const uint32_t * saved, uint32_t count, uint32_t & err )
     {
@@ -1150,92 +1231,60 @@ namespace apo2
                 err |= kErrWalk;
                 break;
             }
-            const uint32_t m    = min( 32u, top );
-            const uint32_t node = lane < m ? frontier[ top - 1 - lane ] : kNone;
+            const uint32_t m = min( 32u * kCoopWidth, top );
+            uint32_t       node[ kCoopWidth ];
+#pragma unroll
+            for ( uint32_t r = 0; r < kCoopWidth; r++ )
+            {
+                const uint32_t q = r * 32 + lane;
+                node[ r ]        = q < m ? frontier[ top - 1 - q ] : kNone;
+            }
             __syncwarp();
-            uint32_t first = 0, second = 0, kids = 0;
-            bool     contrib = false;
-            uint32_t j       = kNone;
-            if ( lane < m && node < n - 1 )
+            uint32_t kids[ kCoopWidth ], first[ kCoopWidth ], second[ kCoopWidth ], jj[ kCoopWidth ];
+            bool     contrib[ kCoopWidth ];
+#pragma unroll
+            for ( uint32_t r = 0; r < kCoopWidth; r++ )
             {
-                Box      lb, rb;
-                uint32_t lc, rc;
-                load_node( c.nodes, node, lb, rb, lc, rc );
-                const float3   closeL = lb.closest( p.bsph ), closeR = rb.closest( p.bsph );
-                const float    dL = lb.distance( p.bsph ), dR = rb.distance( p.bsph );
-                const bool     leftClosest = dL < dR;
-                const float    minFar = leftClosest ? dR : dL, minClose = leftClosest ? dL : dR;
-                const float3   farPoint = leftClosest ? closeR : closeL, closePoint = leftClosest ? closeL : closeR;
-                const uint32_t farChild = leftClosest ? rc : lc, closeChild = leftClosest ? lc : rc;
-                bool           exploreFar = minFar < 0.f;
-                if ( p.hyperbola && exploreFar )
-                    exploreFar = fdot( p.n1, farPoint - p.pp1 ) < 0.f && fdot( p.n2, farPoint - p.pp2 ) < 0.f;
-                bool exploreClose = minClose < 0.f;
-                if ( p.hyperbola && exploreClose )
-                    exploreClose = fdot( p.n1, closePoint - p.pp1 ) < 0.f && fdot( p.n2, closePoint - p.pp2 ) < 0.f;
-                exploreFar   = exploreFar && ( leftClosest ? rb : lb ).distance( p.reach ) < 0.f;
-                exploreClose = exploreClose && ( leftClosest ? lb : rb ).distance( p.reach ) < 0.f;
-                if ( exploreClose )
+                first[ r ] = second[ r ] = 0;
+                ordered_step( c, w, i, si, p, node[ r ], kids[ r ], first[ r ], second[ r ], contrib[ r ], jj[ r ] );
+            }
+            // earliest contributing position of this step
+            uint32_t keep = m, base = top - m;
+#pragma unroll
+            for ( uint32_t r = 0; r < kCoopWidth; r++ )
+            {
+                const uint32_t hits = __ballot_sync( kFull, contrib[ r ] );
+                if ( hits && keep == m )
                 {
-                    first = closeChild;
-                    kids  = 1;
-                    if ( exploreFar )
-                    {
-                        second = farChild;
-                        kids   = 2;
-                    }
-                }
-                else if ( exploreFar )
-                {
-                    first = farChild;
-                    kids  = 1;
+                    const uint32_t q = __ffs( hits ) - 1;
+                    found            = __shfl_sync( kFull, jj[ r ], q );
+                    keep             = r * 32 + q;
+                    base             = 0;
                 }
             }
-            else if ( lane < m && node < 2 * n - 1 )
+            // children of the positions before `keep`, in position order, the earliest on top
+            uint32_t off[ kCoopWidth ], mine[ kCoopWidth ], total = 0;
+#pragma unroll
+            for ( uint32_t r = 0; r < kCoopWidth; r++ )
             {
-                j       = node - ( n - 1 );
-                bool can = j != i && j != p.k && j != p.l && c.status[ j ] != kBuried;
-                double4 sj = make_double4( 0, 0, 0, 0 );
-                if ( can )
-                {
-                    sj              = c.sites[ j ];
-                    const float4 fj = to_float( sj );
-                    can             = intersects( fj, p.bsph ) && flength( f3( fj ) - f3( p.reach ) ) <= p.reach.w;
-                    if ( p.hyperbola )
-                        can = can && double( fdot( p.n1, f3( fj ) - p.pp1 ) ) < -sj.w
-                              && double( fdot( p.n2, f3( fj ) - p.pp2 ) ) < -sj.w;
-                }
-                if ( can )
-                    can = !known_by_lane( w, j );
-                if ( can )
-                {
-                    double4 x0 = make_double4( 0, 0, 0, 0 ), x1 = make_double4( 0, 0, 0, 0 );
-                    const uint32_t mask = quadrisector( si, sj, p.sk, p.sl, x0, x1 );
-                    contrib = mask == 3 && ( clear_by_lane( c, w, x0, p.k, p.l ) || clear_by_lane( c, w, x1, p.k, p.l ) );
-                }
+                mine[ r ]        = r * 32 + lane < keep ? kids[ r ] : 0u;
+                uint32_t round   = 0;
+                off[ r ]         = total + warp_exclusive_scan( mine[ r ], round );
+                total           += round;
             }
-            const uint32_t hits = __ballot_sync( kFull, contrib );
-            uint32_t       keep = m, base = top - m;
-            if ( hits )
-            {
-                const uint32_t q = __ffs( hits ) - 1;
-                found            = __shfl_sync( kFull, j, q );
-                keep             = q;
-                base             = 0;
-            }
-            const uint32_t mine  = lane < keep ? kids : 0u;
-            uint32_t       total = 0;
-            const uint32_t off   = warp_exclusive_scan( mine, total );
             if ( base + total > kCoopCap )
             {
                 err |= kErrStack;
                 break;
             }
-            // the earliest child ends on top
-            if ( mine >= 1 )
-                frontier[ base + total - 1 - off ] = first;
-            if ( mine == 2 )
-                frontier[ base + total - 2 - off ] = second;
+#pragma unroll
+            for ( uint32_t r = 0; r < kCoopWidth; r++ )
+            {
+                if ( mine[ r ] >= 1 )
+                    frontier[ base + total - 1 - off[ r ] ] = first[ r ];
+                if ( mine[ r ] == 2 )
+                    frontier[ base + total - 2 - off[ r ] ] = second[ r ];
+            }
             __syncwarp();
             top = base + total;
         }

@@ -45,9 +45,14 @@ namespace apo2
 
     // Exact edge validation: a lane walks its edge's search alone for kLaneWalk steps; a
     // search still running then is finished by the whole warp, in the same order, from a
-    // frontier of at most kCoopCap nodes kept in global scratch (plus each lane's saved stack).
+    // frontier of at most kCoopCap nodes kept in global scratch (plus each lane's saved stack),
+    // kCoopWidth x 32 frontier nodes per step.
     constexpr uint32_t kLaneWalk         = 256;
-    constexpr uint32_t kCoopCap          = 4096;
+#ifndef APO2_COOP_WIDTH
+#define APO2_COOP_WIDTH 4
+#endif
+    constexpr uint32_t kCoopWidth        = APO2_COOP_WIDTH; // frontier nodes per lane per step
+    constexpr uint32_t kCoopCap          = 8192;
     constexpr uint32_t kWalkScratchWords = kCoopCap + 32 * ( kStack + 1 );
 
     // Position of a stored vertex: root `type` of quadrisector(si, sj, sk, sl) with the
