@@ -95,6 +95,7 @@ SIGNATURES = {
     "apo2_generate_chains": (_I, [_U32, _U32, ctypes.c_double, _U64, _P]),
     "apo2_topology_json": (_I, [_P, _P, _U64, _P]),
     "apo2_certify": (_I, [_P, _P, _P, _U64, _U32, _I, _P, _P]),
+    "apo2_contribution_profile": (_I, [_P, _U32, _P, _P]),
     "apo2_batch_create": (_I, [_U32, _U32, _P, _P]),
     "apo2_batch_build": (_I, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "apo2_batch_destroy": (_I, [_P]),
@@ -178,6 +179,7 @@ class AlgorithmGPU:
         opt.knn_steps = APO2_NO_KNN_STEPS if knnValidationStep == 0 else knnValidationStep
         opt.stop_after = stop_after
         self.knnValidationStep = knnValidationStep
+        self._k = k
         handle = ctypes.c_void_p()
         _check(lib.apo2_create(self._sites.ctypes.data, self.n, dtype, APO2_HOST, ctypes.byref(opt), ctypes.byref(handle)))
         self._h = handle
@@ -250,6 +252,18 @@ class AlgorithmGPU:
         _check(self._lib.apo2_certify(self._h, p.ctypes.data, i.ctypes.data, p.shape[0], arity, APO2_HOST,
                                       flags.ctypes.data, ctypes.byref(bad)))
         return bad.value, flags[:p.shape[0]]
+
+    def contribution_profile(self, steps: int = 4):
+        """Per-rank labels of the kNN cell construction (sorted cell order): (contributed,
+        certified) uint8 arrays of shape (n, steps * k), and the rank at which each cell
+        certified (1-based; 0 if it did not within steps * k neighbours)."""
+        k = self._k
+        contributed = np.zeros((self.n, steps * k), dtype=np.uint8)
+        certified = np.zeros((self.n, steps * k), dtype=np.uint8)
+        _check(self._lib.apo2_contribution_profile(self._h, steps, contributed.ctypes.data, certified.ctypes.data))
+        has = certified.any(axis=1)
+        certified_k = np.where(has, certified.argmax(axis=1) + 1, 0)
+        return contributed, certified, certified_k
 
     def topology_json(self) -> str:
         """The topology as the reference's topology harness writes it (JSON text)."""

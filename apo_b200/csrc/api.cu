@@ -808,6 +808,53 @@ apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint3
     return APO2_OK;
 }
 
+apo2_status apo2_contribution_profile( apo2_handle * h, uint32_t steps, uint8_t * contributed, uint8_t * certified )
+{
+    if ( !h || !contributed || !certified || steps == 0 || steps > 64 )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_contribution_profile" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    const uint32_t n   = h->n;
+    const uint32_t row = steps * h->cells.k;
+    const size_t   bytes = size_t( n ) * row;
+    void *         buf   = nullptr;
+    APO2_CUDA( cudaMalloc( &buf, 2 * bytes ), "profile buffers" );
+    uint8_t * dc = static_cast<uint8_t *>( buf );
+    uint8_t * dr = dc + bytes;
+    cudaMemset( buf, 0, 2 * bytes );
+    {
+        ObserveScope observe( h );
+        h->launches    = 0;
+        h->events_used = 0;
+        h->records.clear();
+        cudaStream_t s = 0;
+        cudaMemsetAsync( h->error, 0, sizeof( uint32_t ), s );
+        launch_bounds( h->input, h->input_f64, n, h->input_d4, h->partials, h->partial_count, h->bounds_counter, h->scene,
+                       h->tree.sites + n, s );
+        launch_tree( h->tree, n, h->input_d4, h->scene, h->sort, s );
+        for ( uint32_t step = 0; step < steps; step++ )
+        {
+            launch_knn( h->cells, step, s );
+            launch_cells_profile( h->cells, step, row, dc, dr, s );
+        }
+    }
+    uint32_t    err = 0;
+    cudaError_t e   = cudaDeviceSynchronize();
+    if ( e == cudaSuccess )
+        e = cudaMemcpy( contributed, dc, bytes, cudaMemcpyDeviceToHost );
+    if ( e == cudaSuccess )
+        e = cudaMemcpy( certified, dr, bytes, cudaMemcpyDeviceToHost );
+    if ( e == cudaSuccess )
+        e = cudaMemcpy( &err, h->error, sizeof( err ), cudaMemcpyDeviceToHost );
+    cudaFree( buf );
+    h->built     = false; // the stores hold the profile run, not a build
+    h->extracted = false;
+    if ( e != cudaSuccess )
+        return cuda_fail( e, "contribution profile" );
+    if ( err )
+        return fail( APO2_ERR_CAPACITY, "capacity flags " + std::to_string( err ) );
+    return APO2_OK;
+}
+
 apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, uint32_t vcap, uint32_t * vcount,
                            uint32_t * edges, uint32_t ecap, uint32_t * ecount )
 {

@@ -909,6 +909,73 @@ namespace apo2
         report( c, err );
     }
 
+    // Per-neighbour labels of the kNN cell construction (the reference's measurement harness
+    // app/benchmarks/benchmark_contributing_nearest.cu:10-129): for each cell and each kNN rank,
+    // whether that neighbour changed the cell and whether the security-radius certificate held
+    // after it. A cell stops at the rank where it certifies (and is then FullyValidated). Row i
+    // of `contributed` / `certified` holds steps x k bytes; this step writes its k.
+    __global__ void __launch_bounds__( kCellBlock, 4 ) k_cells_profile( CellContext c, uint32_t step, uint32_t row,
+                                                                       uint8_t * __restrict__ contributed,
+                                                                       uint8_t * __restrict__ certified )
+    {
+        extern __shared__ __align__( 16 ) unsigned char smem[];
+        const uint32_t warp = threadIdx.x >> 5;
+        WarpCell       w    = carve( smem, warp, 0 );
+        uint32_t       err  = 0;
+        while ( true )
+        {
+            uint32_t i = 0;
+            if ( lane_id() == 0 )
+                i = atomicAdd( c.work_counter, 1u );
+            i = __shfl_sync( kFull, i, 0 );
+            if ( i >= c.n )
+                break;
+            const uint8_t status = c.status[ i ];
+            if ( status == kFullyValidated || ( step > 0 && status == kBuried ) )
+                continue;
+            const double4 si = c.sites[ i ];
+            if ( step > 0 )
+                load_cell( c, w, i, si, true, true );
+            else
+                initial_cell( c, w, si );
+            if ( status == kBuried )
+            {
+                store_cell( c, w, i, 0, err );
+                __syncwarp();
+                continue;
+            }
+            double known = -DBL_MAX;
+            for ( uint32_t q = 0; q < c.k; q++ )
+            {
+                const uint32_t j = c.knn[ size_t( i ) * c.k + q ];
+                if ( j == kNone )
+                    break;
+                if ( c.status[ j ] == kBuried )
+                    continue;
+                const double4 sj      = c.sites[ j ];
+                const bool    changed = update_cell( c, w, i, si, j, sj, err );
+                known                 = fmax( known, sphere_distance( si, sj ) );
+                const double radius   = cell_radius( c, w, si );
+                const bool   over     = gt_eps( known, 2.0 * radius );
+                if ( lane_id() == 0 )
+                {
+                    const size_t at = size_t( row ) * i + size_t( step ) * c.k + q;
+                    contributed[ at ] = changed ? 1 : 0;
+                    certified[ at ]   = over ? 1 : 0;
+                    if ( over )
+                        c.status[ i ] = kFullyValidated;
+                }
+                if ( over )
+                    break;
+            }
+            if ( lane_id() == 0 )
+                c.known_radii[ i ] = float( known );
+            store_cell( c, w, i, 0, err );
+            __syncwarp();
+        }
+        report( c, err );
+    }
+
     // -----------------------------------------------------------------------------------
     // Vertex validation (algorithm.inl:208-476)
     // -----------------------------------------------------------------------------------
@@ -2160,6 +2227,21 @@ namespace apo2
     {
         cudaMemsetAsync( c.work_counter, 0, sizeof( uint32_t ), s );
         APO2_LAUNCH( "k_cells", s, k_cells<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, mode ) );
+    }
+
+    void launch_cells_profile( const CellContext & c, uint32_t step, uint32_t row, uint8_t * contributed, uint8_t * certified,
+                               cudaStream_t s )
+    {
+        configure_cell_kernels();
+        static bool configured = false;
+        if ( !configured )
+        {
+            cudaFuncSetAttribute( k_cells_profile, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( false ) ) );
+            configured = true;
+        }
+        cudaMemsetAsync( c.work_counter, 0, sizeof( uint32_t ), s );
+        APO2_LAUNCH( "k_cells_profile", s,
+                     k_cells_profile<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, step, row, contributed, certified ) );
     }
 
     void launch_tasks( const CellContext & c, uint32_t * tasks, uint32_t * count, cudaStream_t s )

@@ -105,6 +105,9 @@ namespace apo2
     constexpr uint32_t kCellsNext     = 1;
     constexpr uint32_t kCellsInitOnly = 2;
     void launch_knn( const CellContext & c, uint32_t step, cudaStream_t s );
+    // kNN cells with per-rank labels (contribution, certificate), rows of `row` bytes per cell
+    void launch_cells_profile( const CellContext & c, uint32_t step, uint32_t row, uint8_t * contributed, uint8_t * certified,
+                               cudaStream_t s );
     void launch_cells( const CellContext & c, uint32_t mode, cudaStream_t s );
     void launch_tasks( const CellContext & c, uint32_t * tasks, uint32_t * count, cudaStream_t s );
     void launch_vertex_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s );

@@ -178,6 +178,15 @@ apo2_status apo2_topology_json( apo2_handle * h, char * json, uint64_t capacity,
 apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint32_t * ids, uint64_t count, uint32_t arity,
                           apo2_location location, uint8_t * flags, uint64_t * bad );
 
+/* Labels of the kNN cell construction, as the reference's measurement harness records them
+ * (app/benchmarks/benchmark_contributing_nearest.cu:10-129): `steps` kNN steps of the handle's K
+ * neighbours each; for cell i (sorted order, as apo2_debug_array) and rank r < steps * K,
+ * contributed[i * steps * K + r] = 1 when that neighbour changed the cell and certified[...] = 1
+ * when the security-radius certificate held after it; a cell stops at the rank where it
+ * certifies. Both arrays are host buffers of n * steps * K bytes. The run replaces the handle's
+ * stores (build again before reading a diagram). Ranks past a cell's end stay 0. */
+apo2_status apo2_contribution_profile( apo2_handle * h, uint32_t steps, uint8_t * contributed, uint8_t * certified );
+
 /* Per-cell store of one site (given by original id): its vertices as (j, k, l, type) and
  * edges as (j, k, vertex count or 0xffffffff for a closed trisector), ids original. */
 apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, uint32_t vertex_capacity,

@@ -1,0 +1,34 @@
+"""Per-rank kNN labels (apo2_contribution_profile, the reference's contributing-nearest
+harness): a cell certifies within the first K ranks when the build's kNN step leaves it
+FullyValidated, since later neighbours only grow the known radius and shrink the cell (up to
+near-threshold rounding of the certificate, allowed on one cell in a thousand)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("kind", ["uniform", "protein"])
+def test_profile_agrees_with_the_knn_certificate(kind):
+    import apo_b200
+    from apo_b200 import generators as g
+    sites = g.uniform_random(20000, 127.0, 0.5, 2.0, 31) if kind == "uniform" else g.protein_chains(40, 500, 0.01, seed=8)
+    after_knn = apo_b200.AlgorithmGPU(sites, stop_after=1)
+    after_knn.build()
+    status = after_knn.debug_array("status")
+    after_knn.close()
+
+    algo = apo_b200.AlgorithmGPU(sites)
+    contributed, certified, certified_k = algo.contribution_profile(steps=3)
+    assert contributed.shape == (sites.shape[0], 48)
+    live = status != 0xFF
+    agree = ((certified_k[live] >= 1) & (certified_k[live] <= 16)) == (status[live] == 1)
+    assert agree.mean() >= 0.999, int((~agree).sum())
+    # labels stop at the certifying rank, and the first neighbour always cuts the initial cell
+    rows = np.nonzero(certified_k)[0]
+    assert np.all(certified[rows].sum(axis=1) == 1)
+    assert contributed[live, 0].mean() > 0.9
+    # a build after the profile is the normal one
+    algo.build()
+    assert algo.stats()["error_flags"] == 0
+    algo.close()
