@@ -99,6 +99,9 @@ SIGNATURES = {
     "apo2_batch_create": (_I, [_U32, _U32, _P, _P]),
     "apo2_batch_build": (_I, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "apo2_batch_destroy": (_I, [_P]),
+    "apo2_cavity_directions": (_I, [_U32, _P]),
+    "apo2_cavity_hit_ratios": (_I, [_P, _P, _U32, _I, _U32, _P, _U64, _P, _P]),
+    "apo2_cavity_vertices": (_I, [_P, ctypes.c_float, ctypes.c_float, _P, _U64, _P]),
 }
 
 
@@ -265,6 +268,31 @@ class AlgorithmGPU:
         certified_k = np.where(has, certified.argmax(axis=1) + 1, 0)
         return contributed, certified, certified_k
 
+    def cavity_hit_ratios(self, spheres=None, samples: int = 64):
+        """Occlusion of every output vertex (app/cavity/utils.cu:17-63): the share of `samples`
+        Halton-direction rays from the vertex centre that meet a sphere of `spheres` ((m, 4) float
+        x, y, z, r, sphere i standing for site i; default: this diagram's sites in float).
+        Returns (ratios float32[vertices], (tree ms, ray casting ms))."""
+        sph = np.ascontiguousarray(np.asarray(self._sites if spheres is None else spheres, dtype=np.float32).reshape(-1, 4))
+        count = self.output_counts()[0]
+        ratios = np.zeros(max(count, 1), dtype=np.float32)
+        got = ctypes.c_uint64()
+        ms = (ctypes.c_float * 2)()
+        _check(self._lib.apo2_cavity_hit_ratios(self._h, sph.ctypes.data, sph.shape[0], APO2_HOST, samples,
+                                                ratios.ctypes.data, ratios.shape[0], ctypes.byref(got), ms))
+        return ratios[:got.value], (ms[0], ms[1])
+
+    def cavity_vertices(self, hit_ratio_threshold: float = 0.5, radius_threshold: float = 5.0) -> np.ndarray:
+        """Cavity vertices (app/cavity/utils.cu:65-80, 476-509) after cavity_hit_ratios: output
+        vertices with hit ratio and radius above the thresholds, in output order, as (m, 4)
+        float32 (x, y, z, w)."""
+        n = ctypes.c_uint64()
+        _check(self._lib.apo2_cavity_vertices(self._h, hit_ratio_threshold, radius_threshold, None, 0, ctypes.byref(n)))
+        out = np.zeros((max(n.value, 1), 4), dtype=np.float32)
+        _check(self._lib.apo2_cavity_vertices(self._h, hit_ratio_threshold, radius_threshold, out.ctypes.data,
+                                              out.shape[0], ctypes.byref(n)))
+        return out[:n.value]
+
     def topology_json(self) -> str:
         """The topology as the reference's topology harness writes it (JSON text)."""
         n = ctypes.c_uint64()
@@ -377,6 +405,30 @@ def computeApolloniusDiagram(sites) -> VertexDiagram:
         lib.apo2_free(pos)
         lib.apo2_free(ids)
     return VertexDiagram(vertices=p, verticesId=i)
+
+
+def getDirections(count: int = 64) -> np.ndarray:
+    """Ray directions of the cavity detection (app/cavity/utils.cu:288-335): the first `count`
+    points of the Halton sequence on the sphere (bases 2 and 3), unit length, (count, 3) float32."""
+    out = np.zeros((count, 3), dtype=np.float32)
+    _check(load_library().apo2_cavity_directions(count, out.ctypes.data))
+    return out
+
+
+def detect_cavities(sites, trace_spheres=None, hit_ratio_threshold: float = 0.5, radius_threshold: float = 5.0,
+                    samples: int = 64) -> dict:
+    """The reference's cavity application (app/cavity/main.cpp:8-88) without its viewer: the
+    diagram of `sites`, the hit ratio of every vertex against `trace_spheres` (default: `sites`
+    in float; the application traces the sites as loaded and builds the diagram of a joggled
+    copy), and the vertices that pass both thresholds."""
+    algo = AlgorithmGPU(sites)
+    try:
+        algo.build()
+        ratios, ms = algo.cavity_hit_ratios(trace_spheres, samples)
+        cavities = algo.cavity_vertices(hit_ratio_threshold, radius_threshold)
+        return {"hit_ratios": ratios, "cavities": cavities, "ms": ms}
+    finally:
+        algo.close()
 
 
 def computeFullApolloniusDiagram(sites) -> FullDiagram:

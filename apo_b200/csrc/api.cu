@@ -16,6 +16,7 @@
 
 #include "../../include/apo2.h"
 #include "cells.cuh"
+#include "cavity.cuh"
 
 namespace
 {
@@ -88,6 +89,14 @@ struct apo2_handle
     void *        out_alloc = nullptr;
     bool          built     = false;
     bool          extracted = false;
+
+    // cavity detection: hit ratios of the extraction numbered ratio_epoch
+    void *   cavity_alloc  = nullptr;
+    size_t   cavity_bytes  = 0;
+    float *  ratios        = nullptr;
+    uint64_t ratio_count   = 0;
+    uint64_t extract_epoch = 0;
+    uint64_t ratio_epoch   = ~0ull;
 
     cudaEvent_t events[ kStages + 1 ] = {};
     bool        timing                = false;
@@ -248,8 +257,9 @@ namespace
         const cudaError_t err = cudaGetLastError();
         if ( err != cudaSuccess )
             return cuda_fail( err, "build launch" );
-        h->built     = true;
-        h->extracted = false;
+        h->built       = true;
+        h->extracted   = false;
+        h->ratio_epoch = ~0ull; // hit ratios belong to the previous build's vertices
         return APO2_OK;
     }
 
@@ -258,6 +268,7 @@ namespace
         ObserveScope observe( h );
         launch_output( h->cells, h->out, s );
         record( h, 7, s );
+        h->extract_epoch++;
         const cudaError_t err = cudaGetLastError();
         if ( err != cudaSuccess )
             return cuda_fail( err, "output launch" );
@@ -808,6 +819,145 @@ apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint3
     return APO2_OK;
 }
 
+apo2_status apo2_cavity_directions( uint32_t count, float * xyz )
+{
+    if ( !xyz || count == 0 || count > kCavityMaxSamples )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_cavity_directions" );
+    cavity_directions( count, xyz, nullptr );
+    return APO2_OK;
+}
+
+apo2_status apo2_cavity_hit_ratios( apo2_handle * h, const float * spheres, uint32_t sphere_count, apo2_location location,
+                                    uint32_t samples, float * hit_ratios, uint64_t capacity, uint64_t * count, float * ms )
+{
+    if ( !h || !count || ( !spheres && sphere_count ) || samples == 0 || samples > kCavityMaxSamples
+         || ( location != APO2_HOST && location != APO2_DEVICE ) )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_cavity_hit_ratios" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    apo2_status st = settle_output( h, 0 );
+    if ( st != APO2_OK )
+        return st;
+    const uint64_t q = h->stats.output_vertices;
+    if ( hit_ratios && capacity < q )
+    {
+        *count = q;
+        return fail( APO2_ERR_INVALID_ARG, "hit ratio capacity too small" );
+    }
+    if ( q > UINT32_MAX )
+        return fail( APO2_ERR_TOO_LARGE, "more than 2^32 - 1 vertices" );
+    // persistent: ratios, filter offsets and scan sums of q vertices
+    const size_t keep = align256( sizeof( float ) * std::max<uint64_t>( q, 1 ) ) + align256( sizeof( uint32_t ) * std::max<uint64_t>( q, 1 ) )
+                        + align256( sizeof( uint32_t ) * output_scan_scratch_words( uint32_t( q ) ) ) + 256;
+    if ( keep > h->cavity_bytes )
+    {
+        if ( h->cavity_alloc )
+            cudaFree( h->cavity_alloc );
+        h->cavity_alloc = nullptr;
+        h->cavity_bytes = 0;
+        APO2_CUDA( cudaMalloc( &h->cavity_alloc, keep ), "cavity buffers" );
+        h->cavity_bytes = keep;
+    }
+    h->ratios      = static_cast<float *>( h->cavity_alloc );
+    h->ratio_epoch = ~0ull;
+    // per call: the sphere tree, the spheres (host input) and the direction table
+    const size_t tree_bytes  = trace_tree_bytes( sphere_count );
+    const size_t copy_bytes  = location == APO2_HOST ? align256( sizeof( float4 ) * std::max<uint32_t>( sphere_count, 1 ) ) : 0;
+    const size_t dir_bytes   = align256( sizeof( float4 ) * 2 * samples );
+    void *       scratch     = nullptr;
+    APO2_CUDA( cudaMalloc( &scratch, tree_bytes + copy_bytes + dir_bytes ), "cavity scratch" );
+    char *         base  = static_cast<char *>( scratch );
+    float4 *       dirs  = reinterpret_cast<float4 *>( base + tree_bytes + copy_bytes );
+    const float4 * trace = reinterpret_cast<const float4 *>( spheres );
+    std::vector<float> table( 8 * size_t( samples ) );
+    cavity_directions( samples, nullptr, table.data() );
+    cudaEvent_t ev[ 3 ] = {};
+    for ( auto & e : ev )
+        cudaEventCreate( &e );
+    cudaError_t e = cudaSuccess;
+    if ( location == APO2_HOST && sphere_count )
+    {
+        float4 * copy = reinterpret_cast<float4 *>( base + tree_bytes );
+        e             = cudaMemcpyAsync( copy, spheres, sizeof( float4 ) * sphere_count, cudaMemcpyHostToDevice, 0 );
+        trace         = copy;
+    }
+    if ( e == cudaSuccess )
+        e = cudaMemcpyAsync( dirs, table.data(), sizeof( float ) * table.size(), cudaMemcpyHostToDevice, 0 );
+    if ( e == cudaSuccess )
+        e = cudaMemsetAsync( h->error, 0, sizeof( uint32_t ), 0 );
+    if ( e == cudaSuccess )
+    {
+        ObserveScope observe( h );
+        TraceTree    tree;
+        trace_tree_carve( tree, base, sphere_count, h->error );
+        cudaEventRecord( ev[ 0 ], 0 );
+        launch_trace_tree( tree, trace, 0 );
+        cudaEventRecord( ev[ 1 ], 0 );
+        launch_occlusion( tree, trace, h->out.vpos, h->out.vids, q, dirs, samples, h->ratios, h->error, 0 );
+        cudaEventRecord( ev[ 2 ], 0 );
+        e = cudaGetLastError();
+    }
+    if ( e == cudaSuccess )
+        e = cudaStreamSynchronize( 0 );
+    uint32_t err = 0;
+    if ( e == cudaSuccess )
+        e = cudaMemcpy( &err, h->error, sizeof( err ), cudaMemcpyDeviceToHost );
+    if ( e == cudaSuccess && hit_ratios && q )
+        e = cudaMemcpy( hit_ratios, h->ratios, sizeof( float ) * q, cudaMemcpyDeviceToHost );
+    if ( e == cudaSuccess && ms )
+    {
+        cudaEventElapsedTime( &ms[ 0 ], ev[ 0 ], ev[ 1 ] );
+        cudaEventElapsedTime( &ms[ 1 ], ev[ 1 ], ev[ 2 ] );
+    }
+    for ( auto & x : ev )
+        cudaEventDestroy( x );
+    cudaFree( scratch );
+    if ( e != cudaSuccess )
+        return cuda_fail( e, "cavity hit ratios" );
+    if ( err )
+        return fail( APO2_ERR_CAPACITY, "ray walk flags " + std::to_string( err ) );
+    h->ratio_count = q;
+    h->ratio_epoch = h->extract_epoch;
+    *count         = q;
+    return APO2_OK;
+}
+
+apo2_status apo2_cavity_vertices( apo2_handle * h, float hit_ratio_threshold, float radius_threshold, float * xyzw,
+                                  uint64_t capacity, uint64_t * count )
+{
+    if ( !h || !count )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_cavity_vertices" );
+    if ( !h->built || h->ratio_epoch != h->extract_epoch )
+        return fail( APO2_ERR_NOT_BUILT, "no hit ratios for the last build (apo2_cavity_hit_ratios)" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    const uint64_t q       = h->ratio_count;
+    char *         base    = static_cast<char *>( h->cavity_alloc );
+    uint32_t *     offsets = reinterpret_cast<uint32_t *>( base + align256( sizeof( float ) * std::max<uint64_t>( q, 1 ) ) );
+    uint32_t *     sums    = offsets + align256( sizeof( uint32_t ) * std::max<uint64_t>( q, 1 ) ) / sizeof( uint32_t );
+    uint64_t *     total   = reinterpret_cast<uint64_t *>( base + h->cavity_bytes - 256 );
+    float4 *       out     = nullptr;
+    if ( xyzw && capacity )
+        APO2_CUDA( cudaMalloc( &out, sizeof( float4 ) * capacity ), "cavity output" );
+    {
+        ObserveScope observe( h );
+        launch_cavity_filter( h->out.vpos, h->ratios, q, hit_ratio_threshold, radius_threshold, offsets, sums, total, out,
+                              capacity, 0 );
+    }
+    uint64_t    found = 0;
+    cudaError_t e     = cudaGetLastError();
+    if ( e == cudaSuccess )
+        e = cudaMemcpy( &found, total, sizeof( found ), cudaMemcpyDeviceToHost );
+    if ( e == cudaSuccess && out && found )
+        e = cudaMemcpy( xyzw, out, sizeof( float4 ) * std::min( found, capacity ), cudaMemcpyDeviceToHost );
+    if ( out )
+        cudaFree( out );
+    if ( e != cudaSuccess )
+        return cuda_fail( e, "cavity vertices" );
+    *count = found;
+    if ( xyzw && found > capacity )
+        return fail( APO2_ERR_INVALID_ARG, "cavity vertex capacity too small" );
+    return APO2_OK;
+}
+
 apo2_status apo2_contribution_profile( apo2_handle * h, uint32_t steps, uint8_t * contributed, uint8_t * certified )
 {
     if ( !h || !contributed || !certified || steps == 0 || steps > 64 )
@@ -1056,6 +1206,8 @@ apo2_status apo2_destroy( apo2_handle * h )
     cudaDeviceSynchronize();
     if ( h->out_alloc )
         cudaFree( h->out_alloc );
+    if ( h->cavity_alloc )
+        cudaFree( h->cavity_alloc );
     if ( h->arena.base )
         cudaFree( h->arena.base );
     if ( h->timing )

@@ -140,4 +140,12 @@ namespace apo2
     void   launch_lbvh_f32( const float4 * sites, uint32_t n, float3 lo, float3 scale, uint32_t * indices, uint64_t * codes,
                             int32_t * parent, int32_t * left, int32_t * right, float4 * boxes, uint32_t * sizes,
                             uint32_t * arrivals, SortScratch & sort, cudaStream_t s );
+    // Pieces of the tree build for callers that build trees over other sphere sets: Morton
+    // codes inside a box held on the device (lo xyz, 1 / extent xyz), and the Karras
+    // hierarchy, refit and wide-node packing over n Morton-sorted leaves whose boxes are in
+    // boxes[2 (n - 1 + i) + {0, 1}].
+    void launch_morton_box( const float4 * sites, uint32_t n, const float * box, uint64_t * codes, uint32_t * indices,
+                            cudaStream_t s );
+    void launch_hierarchy( const uint64_t * codes, uint32_t n, int32_t * parent, int32_t * left, int32_t * right, float4 * boxes,
+                           uint32_t * arrivals, WideNode * nodes, cudaStream_t s );
 } // namespace apo2

@@ -230,6 +230,20 @@ namespace apo2
         indices[ i ]   = i;
     }
 
+    // Morton codes of float4 sites inside a box held on the device: box[0..2] = lo,
+    // box[3..5] = 1 / extent per axis.
+    __global__ void k_morton_box( const float4 * __restrict__ sites, const float * __restrict__ box, uint32_t n,
+                                  uint64_t * __restrict__ codes, uint32_t * __restrict__ indices )
+    {
+        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        if ( i >= n )
+            return;
+        const float4 s = sites[ i ];
+        codes[ i ]     = morton63( quantize( s.x, box[ 0 ], box[ 3 ] ), quantize( s.y, box[ 1 ], box[ 4 ] ),
+                                   quantize( s.z, box[ 2 ], box[ 5 ] ) );
+        indices[ i ]   = i;
+    }
+
     // ---------------------------------------------------------------------------------
     // Leaves: Morton-order gather of the sites and the leaf boxes (lbvh.cu:88-114)
     // ---------------------------------------------------------------------------------
@@ -411,6 +425,23 @@ namespace apo2
             APO2_LAUNCH( "k_refit", s, k_refit<<<blocks_for( n, 256 ), 256, 0, s>>>( n, t.arrivals, t.parent, t.left, t.right, t.boxes, t.sizes ) );
             APO2_LAUNCH( "k_pack", s, k_pack<<<blocks_for( n - 1, 256 ), 256, 0, s>>>( n, t.left, t.right, t.boxes, t.nodes ) );
         }
+    }
+
+    void launch_morton_box( const float4 * sites, uint32_t n, const float * box, uint64_t * codes, uint32_t * indices,
+                            cudaStream_t s )
+    {
+        APO2_LAUNCH( "k_morton_box", s, k_morton_box<<<blocks_for( n, 256 ), 256, 0, s>>>( sites, box, n, codes, indices ) );
+    }
+
+    void launch_hierarchy( const uint64_t * codes, uint32_t n, int32_t * parent, int32_t * left, int32_t * right, float4 * boxes,
+                           uint32_t * arrivals, WideNode * nodes, cudaStream_t s )
+    {
+        if ( n < 2 )
+            return;
+        APO2_LAUNCH( "k_karras", s, k_karras<<<blocks_for( n - 1, 256 ), 256, 0, s>>>( codes, n, parent, left, right ) );
+        cudaMemsetAsync( arrivals, 0, sizeof( uint32_t ) * ( n - 1 ), s );
+        APO2_LAUNCH( "k_refit", s, k_refit<<<blocks_for( n, 256 ), 256, 0, s>>>( n, arrivals, parent, left, right, boxes, nullptr ) );
+        APO2_LAUNCH( "k_pack", s, k_pack<<<blocks_for( n - 1, 256 ), 256, 0, s>>>( n, left, right, boxes, nodes ) );
     }
 
     void launch_lbvh_f32( const float4 * sites, uint32_t n, float3 lo, float3 scale, uint32_t * indices, uint64_t * codes,

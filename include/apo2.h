@@ -187,6 +187,38 @@ apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint3
  * stores (build again before reading a diagram). Ranks past a cell's end stay 0. */
 apo2_status apo2_contribution_profile( apo2_handle * h, uint32_t steps, uint8_t * contributed, uint8_t * certified );
 
+/* Cavity detection over the diagram, as the reference's cavity application does it
+ * (app/cavity/main.cpp:8-88) with CUDA kernels over a sphere BVH where the reference uses OptiX.
+ *
+ * Directions of the occlusion rays: the first `count` points (1..1024) of the Halton sequence
+ * on the sphere in bases 2 and 3 (Wong, Luk and Heng, "Sampling with Hammersley and Halton
+ * points", 1997) as app/cavity/utils.cu:288-330 generates them, scaled to unit length;
+ * xyz: host float[3 * count]. */
+apo2_status apo2_cavity_directions( uint32_t count, float * xyz );
+
+/* Hit ratio of every output vertex, in apo2_get_vertices order (app/cavity/utils.cu:17-63,
+ * app/cavity/shaders/find_occlusion.cu:26-65): the share of `samples` rays from the vertex centre
+ * (in float), one along each direction of apo2_cavity_directions(samples), that meet a sphere of
+ * `spheres` (float x, y, z, r; host or device) with 0.01 <= t <= 1e16; a ray that starts inside
+ * a sphere meets it where it leaves it. Sphere i stands for the site of original id i (the
+ * reference traces the sites as loaded, before the joggle the diagram was built from). Each
+ * ray / sphere decision is the single-precision test of cavity.cu, so the ratios are exactly
+ * those of testing every ray against every sphere. The ratios stay on the device for
+ * apo2_cavity_vertices; hit_ratios (optional, host, capacity floats) receives a copy and
+ * *count their number. ms (optional, 2 floats) receives the device times of the sphere tree
+ * build and of the ray casting. */
+apo2_status apo2_cavity_hit_ratios( apo2_handle * h, const float * spheres_xyzr, uint32_t sphere_count,
+                                    apo2_location location, uint32_t samples, float * hit_ratios, uint64_t capacity,
+                                    uint64_t * count, float * ms );
+
+/* Cavity vertices (app/cavity/utils.cu:65-80, 476-509): the output vertices whose hit ratio is
+ * above hit_ratio_threshold and whose radius is above radius_threshold (the reference's
+ * application starts at 0.5 and 5), in output order, as float (x, y, z, w). Needs
+ * apo2_cavity_hit_ratios after the last build (APO2_ERR_NOT_BUILT otherwise). xyzw: host
+ * float[4 * capacity], or NULL to count only; *count receives the number found. */
+apo2_status apo2_cavity_vertices( apo2_handle * h, float hit_ratio_threshold, float radius_threshold, float * xyzw,
+                                  uint64_t capacity, uint64_t * count );
+
 /* Per-cell store of one site (given by original id): its vertices as (j, k, l, type) and
  * edges as (j, k, vertex count or 0xffffffff for a closed trisector), ids original. */
 apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, uint32_t vertex_capacity,

@@ -95,3 +95,57 @@ def build(sites: np.ndarray, stage: int = STAGE_OUTPUT, threads: int = 0, k: int
         return out
     finally:
         lib.oracle_free(handle)
+
+
+def _load_cavity():
+    lib = _load()
+    if not getattr(lib, "_cavity_ready", False):
+        lib.oracle_cavity_directions.restype = None
+        lib.oracle_cavity_directions.argtypes = [ctypes.c_uint32, ctypes.c_void_p]
+        lib.oracle_cavity_hit_ratios.restype = None
+        lib.oracle_cavity_hit_ratios.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint32,
+                                                 ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        lib.oracle_cavity_filter.restype = ctypes.c_uint64
+        lib.oracle_cavity_filter.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_float,
+                                             ctypes.c_float, ctypes.c_void_p]
+        lib._cavity_ready = True
+    return lib
+
+
+def cavity_directions(count: int = 64) -> np.ndarray:
+    """Halton ray directions of the cavity detection, (count, 3) float32 (oracle/cavity_oracle.cpp)."""
+    out = np.zeros((count, 3), dtype=np.float32)
+    _load_cavity().oracle_cavity_directions(count, out.ctypes.data)
+    return out
+
+
+def cavity_hit_ratios(vertices, spheres, samples: int = 64, use_tree: bool = True, threads: int = 0) -> np.ndarray:
+    """Hit ratio of each vertex ((q, 4): centre and radius, rounded to float32 as the kernels
+    take them) against the spheres ((m, 4) float32). use_tree=False tests every ray against
+    every sphere (the definition); True walks a CPU sphere tree (same ratios)."""
+    v = np.ascontiguousarray(np.asarray(vertices, dtype=np.float64).reshape(-1, 4).astype(np.float32))
+    s = np.ascontiguousarray(np.asarray(spheres, dtype=np.float32).reshape(-1, 4))
+    out = np.zeros(max(v.shape[0], 1), dtype=np.float32)
+    _load_cavity().oracle_cavity_hit_ratios(v.ctypes.data, v.shape[0], s.ctypes.data, s.shape[0], samples,
+                                            1 if use_tree else 0, threads, out.ctypes.data)
+    return out[:v.shape[0]]
+
+
+def cavity_filter(vertices, ratios, hit_ratio_threshold: float = 0.5, radius_threshold: float = 5.0) -> np.ndarray:
+    """Indices of the cavity vertices (ratio and radius above the thresholds), in order."""
+    v = np.ascontiguousarray(np.asarray(vertices, dtype=np.float64).reshape(-1, 4).astype(np.float32))
+    r = np.ascontiguousarray(np.asarray(ratios, dtype=np.float32))
+    keep = np.zeros(max(v.shape[0], 1), dtype=np.uint64)
+    c = _load_cavity().oracle_cavity_filter(v.ctypes.data, r.ctypes.data, v.shape[0], hit_ratio_threshold,
+                                            radius_threshold, keep.ctypes.data)
+    return keep[:c].astype(np.int64)
+
+
+def joggle(sites: np.ndarray, amount: float) -> np.ndarray:
+    """The reference's joggle (apo/src/core/utils.cpp:15-25) of a float64 copy of `sites`."""
+    lib = _load()
+    lib.oracle_joggle.restype = None
+    lib.oracle_joggle.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double]
+    out = np.ascontiguousarray(np.asarray(sites, dtype=np.float64).reshape(-1, 4)).copy()
+    lib.oracle_joggle(out.ctypes.data, out.shape[0], amount)
+    return out
