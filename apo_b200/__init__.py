@@ -269,7 +269,7 @@ class AlgorithmGPU:
         return contributed, certified, certified_k
 
     def cavity_hit_ratios(self, spheres=None, samples: int = 64):
-        """Occlusion of every output vertex (app/cavity/utils.cu:17-63): the share of `samples`
+        """Occlusion of every output vertex (app/cavity/utils.cu:17-65): the share of `samples`
         Halton-direction rays from the vertex centre that meet a sphere of `spheres` ((m, 4) float
         x, y, z, r, sphere i standing for site i; default: this diagram's sites in float).
         Returns (ratios float32[vertices], (tree ms, ray casting ms))."""
@@ -283,7 +283,7 @@ class AlgorithmGPU:
         return ratios[:got.value], (ms[0], ms[1])
 
     def cavity_vertices(self, hit_ratio_threshold: float = 0.5, radius_threshold: float = 5.0) -> np.ndarray:
-        """Cavity vertices (app/cavity/utils.cu:65-80, 476-509) after cavity_hit_ratios: output
+        """Cavity vertices (app/cavity/utils.cu:67-83, 527-559) after cavity_hit_ratios: output
         vertices with hit ratio and radius above the thresholds, in output order, as (m, 4)
         float32 (x, y, z, w)."""
         n = ctypes.c_uint64()
@@ -408,7 +408,7 @@ def computeApolloniusDiagram(sites) -> VertexDiagram:
 
 
 def getDirections(count: int = 64) -> np.ndarray:
-    """Ray directions of the cavity detection (app/cavity/utils.cu:288-335): the first `count`
+    """Ray directions of the cavity detection (app/cavity/utils.cu:201-242): the first `count`
     points of the Halton sequence on the sphere (bases 2 and 3), unit length, (count, 3) float32."""
     out = np.zeros((count, 3), dtype=np.float32)
     _check(load_library().apo2_cavity_directions(count, out.ctypes.data))

@@ -2,12 +2,13 @@
 // (app/cavity/main.cpp:8-88, app/cavity/utils.cu, app/cavity/shaders/find_occlusion.cu),
 // as CUDA kernels over a BVH of this library where the reference uses OptiX:
 //
-//  - occlusion (utils.cu:17-63, find_occlusion.cu:26-65): from the centre of every output
+//  - occlusion (utils.cu:17-65, find_occlusion.cu:26-69): from the centre of every output
 //    vertex, one ray along each of `samples` fixed directions; the vertex's hit ratio is the
 //    share of rays that meet a sphere of the trace set with 0.01 <= t <= 1e16. A ray that
 //    starts inside a sphere meets it where it leaves it (the reference's sphere geometry is
-//    two-sided: its build input leaves OptiX's single-sided option unset);
-//  - filter (utils.cu:65-80, 476-509): the vertices whose hit ratio and radius exceed two
+//    two-sided: its build input, optix/sphere_module.cu:25-44, leaves OptiX's single-sided
+//    option unset);
+//  - filter (utils.cu:67-83, 244-264, 527-559): the vertices whose hit ratio and radius exceed two
 //    thresholds, in output order, as float (x, y, z, w).
 //
 // Whether one ray meets one sphere is decided by ray_meets_sphere() alone, in single
@@ -28,8 +29,8 @@ namespace apo2
     {
         constexpr uint32_t kOcclusionBlock = 128;
         constexpr uint32_t kTraceStack     = 64;
-        constexpr float    kRayMin         = 0.01f; // find_occlusion.cu:45
-        constexpr float    kRayMax         = 1e16f; // find_occlusion.cu:46
+        constexpr float    kRayMin         = 0.01f; // find_occlusion.cu:49
+        constexpr float    kRayMax         = 1e16f; // find_occlusion.cu:50
 
         // Ray o + t d (d of unit length) against the sphere |x - c| = r. The squared distance
         // from c to the line comes from the component of c - o across d, which keeps the
@@ -268,7 +269,7 @@ namespace apo2
 
     // Points k = 0 .. count-1 of the Halton sequence on the sphere in bases 2 and 3 (T.-T. Wong,
     // W.-S. Luk, P.-A. Heng, "Sampling with Hammersley and Halton points", J. Graphics Tools 2(2),
-    // 1997), in the single precision of the reference's generator (app/cavity/utils.cu:288-330,
+    // 1997), in the single precision of the reference's generator (app/cavity/utils.cu:201-242,
     // including its angle of 4 pi times the base-3 radical inverse and its pi of 3.1415926535),
     // then scaled to unit length. dirs4 receives the directions (w = 0) and then their
     // reciprocals, a zero component standing as 1e-20 with its sign.

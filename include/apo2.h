@@ -192,12 +192,12 @@ apo2_status apo2_contribution_profile( apo2_handle * h, uint32_t steps, uint8_t 
  *
  * Directions of the occlusion rays: the first `count` points (1..1024) of the Halton sequence
  * on the sphere in bases 2 and 3 (Wong, Luk and Heng, "Sampling with Hammersley and Halton
- * points", 1997) as app/cavity/utils.cu:288-330 generates them, scaled to unit length;
+ * points", 1997) as app/cavity/utils.cu:201-242 generates them, scaled to unit length;
  * xyz: host float[3 * count]. */
 apo2_status apo2_cavity_directions( uint32_t count, float * xyz );
 
-/* Hit ratio of every output vertex, in apo2_get_vertices order (app/cavity/utils.cu:17-63,
- * app/cavity/shaders/find_occlusion.cu:26-65): the share of `samples` rays from the vertex centre
+/* Hit ratio of every output vertex, in apo2_get_vertices order (app/cavity/utils.cu:17-65,
+ * app/cavity/shaders/find_occlusion.cu:26-69): the share of `samples` rays from the vertex centre
  * (in float), one along each direction of apo2_cavity_directions(samples), that meet a sphere of
  * `spheres` (float x, y, z, r; host or device) with 0.01 <= t <= 1e16; a ray that starts inside
  * a sphere meets it where it leaves it. Sphere i stands for the site of original id i (the
@@ -211,7 +211,7 @@ apo2_status apo2_cavity_hit_ratios( apo2_handle * h, const float * spheres_xyzr,
                                     apo2_location location, uint32_t samples, float * hit_ratios, uint64_t capacity,
                                     uint64_t * count, float * ms );
 
-/* Cavity vertices (app/cavity/utils.cu:65-80, 476-509): the output vertices whose hit ratio is
+/* Cavity vertices (app/cavity/utils.cu:67-83, 244-264, 527-559): the output vertices whose hit ratio is
  * above hit_ratio_threshold and whose radius is above radius_threshold (the reference's
  * application starts at 0.5 and 5), in output order, as float (x, y, z, w). Needs
  * apo2_cavity_hit_ratios after the last build (APO2_ERR_NOT_BUILT otherwise). xyzw: host

@@ -3,16 +3,16 @@
 //
 // Restates the reference's cavity application (app/cavity/main.cpp:8-88):
 //   - ray directions: the Halton sequence on the sphere in bases 2 and 3 (Wong, Luk and Heng,
-//     "Sampling with Hammersley and Halton points", 1997) as app/cavity/utils.cu:288-330
+//     "Sampling with Hammersley and Halton points", 1997) as app/cavity/utils.cu:201-242
 //     generates it in single precision, scaled to unit length;
-//   - occlusion (app/cavity/utils.cu:17-63, app/cavity/shaders/find_occlusion.cu:26-65): the
+//   - occlusion (app/cavity/utils.cu:17-65, app/cavity/shaders/find_occlusion.cu:26-69): the
 //     share of rays from a vertex centre that meet a sphere with 0.01 <= t <= 1e16, a ray from
 //     inside a sphere meeting it where it leaves it. The reference traces with OptiX's sphere
 //     intersector, whose arithmetic is not published; this oracle and the CUDA kernels both
 //     decide each ray / sphere pair with the same single-precision test (component of c - o
 //     across the ray, every operation rounded on its own; compiled with -ffp-contract=off), so
 //     GPU and oracle agree bit for bit while the reference's OptiX run is not reproducible here;
-//   - filter (app/cavity/utils.cu:65-80, 476-509): hit ratio and radius above two thresholds.
+//   - filter (app/cavity/utils.cu:67-83, 244-264, 527-559): hit ratio and radius above two thresholds.
 //
 // Two forms of the occlusion: every ray against every sphere (the definition), and a CPU
 // sphere tree (median splits, boxes padded beyond the test's rounding, any-hit walk) that
@@ -37,7 +37,7 @@ namespace
         float x, y, z, w;
     };
 
-    // find_occlusion.cu:41-50 (tmin 0.01, tmax 1e16), two-sided sphere
+    // find_occlusion.cu:46-58 (tmin 0.01, tmax 1e16), two-sided sphere
     bool meets( F3 o, F3 d, F4 s )
     {
         const float ox = s.x - o.x, oy = s.y - o.y, oz = s.z - o.z;
@@ -244,7 +244,7 @@ void oracle_cavity_hit_ratios( const float * vertices, uint64_t nv, const float 
 }
 
 // Cavity vertices: indices of the vertices with ratio > ratio_min and w > radius_min, in
-// order; returns their number (app/cavity/utils.cu:476-509).
+// order; returns their number (app/cavity/utils.cu:527-559).
 uint64_t oracle_cavity_filter( const float * vertices, const float * ratios, uint64_t nv, float ratio_min, float radius_min,
                                uint64_t * keep )
 {

@@ -1,7 +1,7 @@
 """Cavity detection on the CPU: the ray directions against the published Halton construction,
 the ray / sphere decision on hand-made scenes, the oracle's sphere tree against its every-ray-
-every-sphere definition, and the filter (app/cavity/utils.cu:17-80, 288-335, 476-509;
-app/cavity/shaders/find_occlusion.cu:26-65)."""
+every-sphere definition, and the filter (app/cavity/utils.cu:17-83, 201-264, 527-559;
+app/cavity/shaders/find_occlusion.cu:26-69)."""
 import math
 
 import numpy as np
