@@ -197,9 +197,77 @@ def cpu_sample(sites: np.ndarray, sample: int, threads: int = 0) -> tuple[float,
     return sample / dt, used, dt, sample
 
 
+def run_reference_cavity(args):
+    """Reference arm of the cavity workload: the reference traces with OptiX (absent, and B200 has
+    no RT cores), so the CPU restatement (oracle sphere tree, all host threads) stands in: each
+    step traces 64 rays from every vertex of the diagram of a central 20,000-site sub-cube
+    (built once, untimed) against all the workload's spheres."""
+    from oracle import oracle as O
+    sites, cfg = workload("protein1m", args.sites)
+    spheres = np.ascontiguousarray(sites.astype(np.float32))
+    sub = spatial_sample(sites, 20000)
+    verts = O.build(sub, O.STAGE_OUTPUT)["out_vertices"].reshape(-1, 4)
+    for _ in range(args.warmup):
+        O.cavity_hit_ratios(verts[:2000], spheres, 64)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.cavity_hit_ratios(verts, spheres, 64)
+        times.append(time.perf_counter() - t0)
+    t = statistics.mean(times)
+    rays = verts.shape[0] * 64
+    value = rays / t
+    cores = os.cpu_count() or 1
+    line = {
+        "impl": "reference", "metric": "occlusion rays/s", "value": value, "unit": "rays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": dict(cfg, workload="cavity detection over the protein-like packing", sample_vertices=int(verts.shape[0]),
+                       note="reference traces with OptiX (SDK absent); CPU restatement (oracle/) of its ray casting"),
+        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": cores, "kind": "port",
+                         "sample": f"{verts.shape[0]} vertices of a central 20,000-site sub-cube's diagram x 64 rays per step"},
+        "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
     """Reference arm: the CPU restatement of the path on a bounded sample, all host threads."""
     if rank != 0:
+        return
+    if args.workload == "cavity":
+        run_reference_cavity(args)
+        return
+    if args.workload == "batch":
+        # the sets of the batch, one diagram after another, until about --cpu-sample sites
+        sets = batch_sets(args.sets, 200, 50000)
+        take, total = [], 0
+        for d in sets:
+            if total >= args.cpu_sample:
+                break
+            take.append(d)
+            total += int(d.shape[0])
+        from oracle import oracle as O
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            for d in take:
+                O.build(d)
+            times.append(time.perf_counter() - t0)
+        t = statistics.mean(times)
+        value = total / t
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"batched protein-like sets ({args.sets}, sizes log-uniform 200-50000)",
+                       "sample_sets": len(take), "sample_sites": total,
+                       "note": "reference has no CPU path; CPU restatement of it (oracle/), one set after another"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                             "sample": f"the first {len(take)} sets ({total} sites), one diagram after another"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
         return
     sites, cfg = workload(args.workload, args.sites)
     sample = min(args.cpu_sample, sites.shape[0])
