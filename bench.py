@@ -497,6 +497,11 @@ def run_batch(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes per output vertex of one k_occlusion launch (ncu, 100,000-site protein-like packing:
+# 46.47 MB for 668,054 vertices)
+OCCLUSION_TRAFFIC_PER_VERTEX = 46.47e6 / 668054
+
+
 def run_cavity(args, world, rank, local):
     """Cavity detection over the protein-like diagram (the reference's cavity application,
     app/cavity/main.cpp:8-88): one step = the sphere tree of the trace spheres, 64 occlusion rays
@@ -575,7 +580,9 @@ def run_cavity(args, world, rank, local):
     achieved = b_alg / (ray_avg / 1e3) / 1e9
     roofline = {
         "bound": "hbm", "kernel": "k_occlusion", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-        "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_kind": peaks_kind,
+        "frac": achieved / peaks["hbm_gbs"], "traffic": OCCLUSION_TRAFFIC_PER_VERTEX * q, "peak_kind": peaks_kind,
+        "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the 100k-site packing "
+                        "(69.6 B per vertex), scaled by vertices",
         "kernel_avg_launch_ms": ray_avg, "tree_ms": float(np.mean(tree_ms)),
         "note": "BVH ray walks over an L2-resident tree: latency-bound, not HBM-bound; rays/s is the figure of merit",
         "algorithmic_bytes_per_launch": b_alg,
