@@ -46,7 +46,8 @@ class Apo2Error(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("k", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32),
                 ("device", ctypes.c_uint32), ("stage_timing", ctypes.c_uint32), ("edge_search", ctypes.c_uint32),
-                ("knn_steps", ctypes.c_uint32), ("stop_after", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 8)]
+                ("knn_steps", ctypes.c_uint32), ("stop_after", ctypes.c_uint32), ("shard_index", ctypes.c_uint32),
+                ("shard_count", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
 
 
 class Stats(ctypes.Structure):
@@ -168,7 +169,10 @@ class AlgorithmGPU:
     """Counterpart of `apo::gpu::AlgorithmGPU<K>` (algorithm.cuh:12-46)."""
 
     def __init__(self, sites, knnValidationStep: int = 1, k: int = 16, max_iterations: int = 10, device: int = 0,
-                 stage_timing: bool = False, edge_search: int = 0, stop_after: int = 0):
+                 stage_timing: bool = False, edge_search: int = 0, stop_after: int = 0, shard: tuple[int, int] = (0, 1)):
+        """`shard` = (index, count): build only the cells of one of `count` contiguous Morton
+        ranges of the sites (one diagram over several GPUs); the shards' outputs, concatenated in
+        shard order, are the whole diagram's."""
         lib = load_library()
         self._sites, dtype = _as_sites(sites)
         self.n = int(self._sites.shape[0])
@@ -181,6 +185,7 @@ class AlgorithmGPU:
         opt.edge_search = edge_search
         opt.knn_steps = APO2_NO_KNN_STEPS if knnValidationStep == 0 else knnValidationStep
         opt.stop_after = stop_after
+        opt.shard_index, opt.shard_count = int(shard[0]), int(shard[1])
         self.knnValidationStep = knnValidationStep
         self._k = k
         handle = ctypes.c_void_p()

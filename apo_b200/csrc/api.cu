@@ -391,6 +391,8 @@ namespace
         CellContext & c   = h->cells;
         c.n               = n;
         c.k               = opt.k;
+        c.lo              = uint32_t( uint64_t( n ) * opt.shard_index / opt.shard_count );
+        c.hi              = uint32_t( uint64_t( n ) * ( opt.shard_index + 1 ) / opt.shard_count );
         c.sites           = t.sites;
         c.sites_f         = t.sites_f;
         c.nodes           = t.nodes;
@@ -446,6 +448,10 @@ namespace
         else if ( opt.knn_steps > 64 )
             return fail( APO2_ERR_INVALID_ARG, "knn_steps is at most 64" );
         opt.max_iterations = std::min( opt.max_iterations, 64u );
+        if ( opt.shard_count == 0 )
+            opt.shard_count = 1;
+        if ( opt.shard_index >= opt.shard_count )
+            return fail( APO2_ERR_INVALID_ARG, "shard_index must be below shard_count" );
         return APO2_OK;
     }
 } // namespace
@@ -633,7 +639,7 @@ namespace
     std::vector<std::pair<uint32_t, uint32_t>> bis;
     std::vector<std::tuple<uint32_t, uint32_t>> tris;
     std::vector<std::tuple<uint32_t, uint32_t, uint32_t>> quads;
-    for ( uint32_t i = 0; i < n; i++ )
+    for ( uint32_t i = h->cells.lo; i < h->cells.hi; i++ ) // this shard's cells
     {
         bis.clear();
         tris.clear();
@@ -1017,6 +1023,8 @@ apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, 
     uint32_t   sorted = 0;
     while ( sorted < h->n && ix[ sorted ] != site )
         sorted++;
+    if ( sorted < h->cells.lo || sorted >= h->cells.hi )
+        return fail( APO2_ERR_INVALID_ARG, "the site's cell belongs to another shard" );
     uint32_t vn = 0, en = 0;
     cudaMemcpy( &vn, h->cells.vertex_nb + sorted, 4, cudaMemcpyDeviceToHost );
     cudaMemcpy( &en, h->cells.edge_nb + sorted, 4, cudaMemcpyDeviceToHost );
@@ -1131,13 +1139,13 @@ apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
     s.buried = 0;
     s.vertex_records = 0;
     s.edge_records   = 0;
-    for ( uint32_t i = 0; i < n; i++ )
+    for ( uint32_t i = h->cells.lo; i < h->cells.hi; i++ ) // this shard's cells
     {
         s.buried += status[ i ] == kBuried;
         s.vertex_records += vnb[ i ];
         s.edge_records += enb[ i ];
     }
-    s.certified_after_knn = n - s.buried - counts[ 0 ];
+    s.certified_after_knn = ( h->cells.hi - h->cells.lo ) - s.buried - counts[ 0 ];
     s.validation_rounds   = 0;
     for ( uint32_t r = 0; r < h->options.max_iterations; r++ )
         s.validation_rounds += counts[ r ] != 0;
@@ -1417,6 +1425,8 @@ apo2_status apo2_batch_create( uint32_t max_sites, uint32_t streams, const apo2_
     const apo2_status ost = normalize_options( options, opt );
     if ( ost != APO2_OK )
         return ost;
+    if ( opt.shard_count != 1 )
+        return fail( APO2_ERR_INVALID_ARG, "a batch builds whole diagrams (shard_count 0 or 1)" );
     opt.stage_timing = 0;
     APO2_CUDA( cudaSetDevice( int( opt.device ) ), "cudaSetDevice" );
     configure_cell_kernels();

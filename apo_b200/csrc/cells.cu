@@ -853,9 +853,9 @@ namespace apo2
         {
             uint32_t i = 0;
             if ( lane_id() == 0 )
-                i = atomicAdd( c.work_counter, 1u );
+                i = c.lo + atomicAdd( c.work_counter, 1u );
             i = __shfl_sync( kFull, i, 0 );
-            if ( i >= c.n )
+            if ( i >= c.hi )
                 break;
             if ( mode == kCellsInitOnly )
             {
@@ -926,9 +926,9 @@ namespace apo2
         {
             uint32_t i = 0;
             if ( lane_id() == 0 )
-                i = atomicAdd( c.work_counter, 1u );
+                i = c.lo + atomicAdd( c.work_counter, 1u );
             i = __shfl_sync( kFull, i, 0 );
-            if ( i >= c.n )
+            if ( i >= c.hi )
                 break;
             const uint8_t status = c.status[ i ];
             if ( status == kFullyValidated || ( step > 0 && status == kBuried ) )
@@ -1715,9 +1715,9 @@ namespace apo2
         {
             uint32_t i = 0;
             if ( lane == 0 )
-                i = atomicAdd( next, 1u );
+                i = c.lo + atomicAdd( next, 1u );
             i = __shfl_sync( kFull, i, 0 );
-            if ( i >= n )
+            if ( i >= c.hi )
                 break;
             if ( c.status[ i ] == kBuried )
                 continue;
@@ -1966,11 +1966,11 @@ namespace apo2
     // Validation task lists on the device (replaces thrust::count / copy_if,
     // algorithm.inl:1551-1583)
     // -----------------------------------------------------------------------------------
-    __global__ void k_tasks( const uint8_t * __restrict__ status, uint32_t n, uint32_t * __restrict__ tasks,
+    __global__ void k_tasks( const uint8_t * __restrict__ status, uint32_t lo, uint32_t hi, uint32_t * __restrict__ tasks,
                              uint32_t * __restrict__ count )
     {
-        const uint32_t i    = blockIdx.x * blockDim.x + threadIdx.x;
-        const bool     open = i < n && status[ i ] == kInValidation;
+        const uint32_t i    = lo + blockIdx.x * blockDim.x + threadIdx.x;
+        const bool     open = i < hi && status[ i ] == kInValidation;
         const uint32_t bal  = __ballot_sync( kFull, open );
         uint32_t       base = 0;
         if ( lane_id() == 0 && bal )
@@ -2001,7 +2001,7 @@ namespace apo2
         for ( uint32_t i = gwarp; i < c.n; i += nwarp )
         {
             uint32_t vc = 0, cc = 0;
-            if ( c.status[ i ] != kBuried )
+            if ( i >= c.lo && i < c.hi && c.status[ i ] != kBuried )
             {
                 const uint32_t vn = c.vertex_nb[ i ], en = c.edge_nb[ i ];
                 for ( uint32_t v = lane; v < vn; v += 32 )
@@ -2028,7 +2028,7 @@ namespace apo2
         const uint32_t lane  = lane_id();
         for ( uint32_t i = gwarp; i < c.n; i += nwarp )
         {
-            if ( c.status[ i ] == kBuried )
+            if ( i < c.lo || i >= c.hi || c.status[ i ] == kBuried )
                 continue;
             const double4  si = c.sites[ i ];
             const uint32_t gi = c.indices[ i ];
@@ -2247,7 +2247,7 @@ namespace apo2
     void launch_tasks( const CellContext & c, uint32_t * tasks, uint32_t * count, cudaStream_t s )
     {
         cudaMemsetAsync( count, 0, sizeof( uint32_t ), s );
-        APO2_LAUNCH( "k_tasks", s, k_tasks<<<( c.n + 255 ) / 256, 256, 0, s>>>( c.status, c.n, tasks, count ) );
+        APO2_LAUNCH( "k_tasks", s, k_tasks<<<std::max( 1u, ( c.hi - c.lo + 255 ) / 256 ), 256, 0, s>>>( c.status, c.lo, c.hi, tasks, count ) );
     }
 
     void launch_vertex_validation( const CellContext & c, const uint32_t * tasks, const uint32_t * count, cudaStream_t s )

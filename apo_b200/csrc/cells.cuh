@@ -26,6 +26,7 @@ namespace apo2
     struct CellContext
     {
         uint32_t         n = 0, k = 16;
+        uint32_t         lo = 0, hi = 0; // cells built: sorted ids [lo, hi) (a shard of the diagram)
         const double4 *  sites   = nullptr; // n + 6, Morton order then the artificial sites
         const float4 *   sites_f = nullptr; // n
         const WideNode * nodes   = nullptr;

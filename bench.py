@@ -138,8 +138,9 @@ class ClockSampler:
 
 
 def dist_setup(backend: str = "nccl"):
-    """One process per GPU (torchrun env). The path does not shard: every rank builds its own
-    replica of the workload, and the only collectives are the timing barrier and max."""
+    """One process per GPU (torchrun env). By default every rank builds its own replica of the
+    workload; with --shard the ranks split one diagram's cells (or the batch's sets). Either way
+    the only collectives are the timing barrier, the max over ranks and byte sums."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -167,6 +168,25 @@ def aggregate_rate(n: int, ms: float, world: int, device) -> tuple[float, float]
     rank's time. Returns (sites/s, max ms)."""
     ms_max = reduce_max(ms, world, device)
     return world * n / (ms_max / 1e3), ms_max
+
+
+def shard_rate(n: int, ms: float, world: int, device) -> tuple[float, float]:
+    """Sites/s of one n-site diagram split into `world` shards (one per rank): n over the
+    slowest rank's time. Returns (sites/s, max ms)."""
+    ms_max = reduce_max(ms, world, device)
+    return n / (ms_max / 1e3), ms_max
+
+
+def reduce_sum(value: float, world: int, device) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    if dist.get_backend() == "gloo":
+        device = "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
 
 
 def barrier(world: int):
@@ -305,7 +325,9 @@ def run_ours(args, world, rank, local):
     peaks, peaks_kind = load_peaks()
 
     # --- device-resident build (value) ---
-    algo = apo_b200.AlgorithmGPU(sites, device=local, stage_timing=False)
+    # --shard: one diagram split over the ranks (each builds one Morton range of cells)
+    shard = (rank, world) if args.shard else (0, 1)
+    algo = apo_b200.AlgorithmGPU(sites, device=local, stage_timing=False, shard=shard)
     stream = 0  # legacy default stream: every launch and event below is on it
     for _ in range(args.warmup):
         algo.build_and_extract(stream)
@@ -325,7 +347,7 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
     barrier(world)
     ms = start.elapsed_time(stop) / args.steps
-    value, ms_max = aggregate_rate(n, ms, world, device)
+    value, ms_max = (shard_rate if args.shard else aggregate_rate)(n, ms, world, device)
     err = algo.stats()["error_flags"]
     # interval certificate of every output vertex (the reference's precision check, on the GPU)
     t_c = time.perf_counter()
@@ -333,7 +355,7 @@ def run_ours(args, world, rank, local):
     certificate = {"vertices": int(vcount), "bad": int(bad_vertices), "seconds": round(time.perf_counter() - t_c, 3)}
 
     # --- per-kernel times of one more build (events around every launch) ---
-    prof_algo = apo_b200.AlgorithmGPU(sites, device=local, stage_timing=True)
+    prof_algo = apo_b200.AlgorithmGPU(sites, device=local, stage_timing=True, shard=shard)
     prof_algo.build_and_extract(stream)
     prof_algo.output_counts()
     prof = prof_algo.kernel_profile()
@@ -400,9 +422,12 @@ def run_ours(args, world, rank, local):
     e1.record()
     torch.cuda.synchronize()
     barrier(world)
-    e2e_value, e2e_ms = aggregate_rate(n, e0.elapsed_time(e1) / e2e_steps, world, device)
-    e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(16 * n),
-           "d2h_bytes_per_step": int(48 * written.value), "ms_per_step": e2e_ms, "steps": e2e_steps}
+    e2e_value, e2e_ms = (shard_rate if args.shard else aggregate_rate)(n, e0.elapsed_time(e1) / e2e_steps, world, device)
+    d2h_job = reduce_sum(48.0 * written.value, world, device)
+    e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(16 * n * world),
+           "d2h_bytes_per_step": int(d2h_job), "ms_per_step": e2e_ms, "steps": e2e_steps,
+           "bytes": "whole job: every rank uploads all sites and downloads its vertices"}
+    vertices_job = int(reduce_sum(float(vcount), world, device)) if args.shard else int(vcount)
     algo.close()
 
     if rank != 0:
@@ -417,11 +442,12 @@ def run_ours(args, world, rank, local):
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": dict(cfg, form="plain (FP64 solves, reference topology)", parallelism=f"replicas{world}",
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "strong" if args.shard else "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(cfg, form="plain (FP64 solves, reference topology)",
+                       parallelism=f"shards{world}" if args.shard else f"replicas{world}",
                        l2="per-cell stores of several GB per diagram are rewritten every step (inputs >> 126 MB L2)",
-                       vertices=int(vcount), closed_edges=int(ccount), error_flags=int(err),
+                       vertices=vertices_job, closed_edges=int(ccount), error_flags=int(err),
                        validation_rounds=int(stats["validation_rounds"])),
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(), "gpu_launches": launches * args.steps,
         "certificate": certificate,
@@ -439,6 +465,18 @@ def batch_sets(count: int, lo: int, hi: int, seed: int = 3):
     return [g.protein_chains(max(1, int(s) // 100), 100, 0.01, seed=int(seed * 100003 + d)) for d, s in enumerate(sizes)]
 
 
+def split_sets(sizes, world: int) -> list[list[int]]:
+    """Size-balanced split of site sets over ranks: largest first, each to the rank with the
+    fewest sites so far (ties to the lower rank). Returns each rank's set indices, ascending."""
+    load = [0] * world
+    share: list[list[int]] = [[] for _ in range(world)]
+    for d in sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i)):
+        r = min(range(world), key=lambda x: (load[x], x))
+        share[r].append(d)
+        load[r] += int(sizes[d])
+    return [sorted(x) for x in share]
+
+
 def run_batch(args, world, rank, local):
     """Batched form: `--sets` protein-like sets of log-uniform size, one step = all of them
     through apo2_batch_build. Timed on the host around a device-synchronised call (the work
@@ -447,8 +485,13 @@ def run_batch(args, world, rank, local):
 
     import apo_b200
     torch.cuda.set_device(local)
-    sets = batch_sets(args.sets, 200, 50000)
-    total = sum(int(d.shape[0]) for d in sets)
+    all_sets = batch_sets(args.sets, 200, 50000)
+    total = sum(int(d.shape[0]) for d in all_sets)
+    # --shard: the sets are split over the ranks (size-balanced), otherwise every rank builds all
+    sets = ([all_sets[i] for i in split_sets([d.shape[0] for d in all_sets], world)[rank]]
+            if args.shard and world > 1 else all_sets)
+    if not sets:
+        raise SystemExit("fewer site sets than ranks")
     batch = apo_b200.Batch(max(int(d.shape[0]) for d in sets), streams=args.streams, device=local)
     for _ in range(args.warmup):
         batch.build(sets, vertices=False)
@@ -461,13 +504,14 @@ def run_batch(args, world, rank, local):
         lat.append(ms)
     torch.cuda.synchronize()
     step = (time.perf_counter() - t0) / args.steps
-    value, ms_max = aggregate_rate(total, step * 1e3, world, "cuda")
+    value, ms_max = (shard_rate if args.shard else aggregate_rate)(total, step * 1e3, world, "cuda")
     lat = np.concatenate(lat)
     # end to end: the vertices of every diagram downloaded too
+    barrier(world)
     t1 = time.perf_counter()
     out, counts, _ = batch.build(sets, vertices=True)
-    e2e_s = time.perf_counter() - t1
-    vertices = int(counts.sum())
+    e2e_s = reduce_max(time.perf_counter() - t1, world, "cuda")
+    vertices = int(reduce_sum(float(counts.sum()), world, "cuda")) if args.shard else int(counts.sum())
     del out
     # the same sets one diagram at a time through the single-diagram API (first 256 sets)
     t2 = time.perf_counter()
@@ -484,15 +528,16 @@ def run_batch(args, world, rank, local):
         return
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "strong" if args.shard else "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"batched protein-like sets ({args.sets}, sizes log-uniform 200-50000)", "sites": total,
                    "streams": args.streams, "vertices": vertices, "timing": "host clock around synchronised batch calls",
-                   "parallelism": f"replicas{world}"},
+                   "parallelism": (f"sets split over {world} ranks" if args.shard else f"replicas{world}")},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "loop_of_single_builds": {"value": loop_rate, "unit": UNIT, "sets": min(256, len(sets))},
-        "e2e": {"value": total / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(16 * total),
-                "d2h_bytes_per_step": int(48 * vertices)},
+        "e2e": {"value": (1 if args.shard else world) * total / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": int(16 * total * (1 if args.shard else world)),
+                "d2h_bytes_per_step": int(48 * vertices * (1 if args.shard else world))},
     }
     print(json.dumps(line), flush=True)
 
@@ -626,6 +671,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--sets", type=int, default=4096, help="batch workload: number of site sets")
     ap.add_argument("--streams", type=int, default=8, help="batch workload: concurrent workers")
+    ap.add_argument("--shard", action="store_true",
+                    help="N>1: one diagram split over the ranks (Morton ranges of cells) instead of N replicas")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

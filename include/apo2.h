@@ -76,7 +76,14 @@ typedef struct apo2_options
     uint32_t stop_after;           /* parity checks only: 0 = the whole build; 1 = stop after the kNN
                                       cell construction; 2 + 2r / 3 + 2r = stop after the vertex / edge
                                       validation of round r (0-based). Output extraction still works */
-    uint32_t reserved[ 8 ];
+    uint32_t shard_index;          /* one diagram over several GPUs: this handle builds the cells of
+                                      shard shard_index of shard_count (shard_count 0 = 1: the whole
+                                      diagram), a contiguous range of the Morton-sorted sites. Every
+                                      shard needs all the sites; its output is its cells' share of the
+                                      diagram's, and the shards' outputs in shard order are the whole
+                                      diagram's output, in order */
+    uint32_t shard_count;
+    uint32_t reserved[ 6 ];
 } apo2_options;
 
 #define APO2_NO_KNN_STEPS 0xffffffffu

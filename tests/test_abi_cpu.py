@@ -63,6 +63,14 @@ def test_host_argument_checks_without_device(lib):
     assert lib.apo2_batch_create(1, 4, None, None) == 1
     assert lib.apo2_batch_build(None, None, None, 0, None, None, None, None) == 1
     assert lib.apo2_batch_destroy(None) == 0
+    # a shard index at or past the shard count is rejected before any CUDA call
+    opt = apo_b200.Options()
+    opt.struct_size = ctypes.sizeof(apo_b200.Options)
+    opt.shard_index, opt.shard_count = 3, 3
+    sites = (ctypes.c_float * 16)()
+    handle = ctypes.c_void_p()
+    assert lib.apo2_create(sites, 4, apo_b200.APO2_F32, apo_b200.APO2_HOST, ctypes.byref(opt), ctypes.byref(handle)) == 1
+    assert b"shard" in lib.apo2_last_error_string()
     keys = ctypes.c_void_p(16)
     assert lib.apo2_radix_sort_pairs_static(keys, keys, (1 << 20) + 1, None) == 7  # APO2_ERR_TOO_LARGE
     assert lib.apo2_radix_sort_scratch_bytes(1 << 20) + 256 <= 256 + 12853760 + 4096
