@@ -335,9 +335,22 @@ const char * apo2_last_error_string( void ) { return g_last_error.c_str(); }
 
 namespace
 {
-    // Device bytes of a handle for n sites (every array of the build, carved from one block).
+    // The cells a handle builds: shard shard_index of shard_count contiguous ranges of the
+    // Morton-sorted sites.
+    void shard_range( uint32_t n, const apo2_options & opt, uint32_t & lo, uint32_t & hi )
+    {
+        const uint32_t count = std::max( opt.shard_count, 1u );
+        lo                   = uint32_t( uint64_t( n ) * opt.shard_index / count );
+        hi                   = uint32_t( uint64_t( n ) * ( opt.shard_index + 1 ) / count );
+    }
+
+    // Device bytes of a handle for n sites (every array of the build, carved from one block;
+    // the per-cell stores only for the shard's cells).
     size_t arena_bytes( uint32_t n, const apo2_options & opt, bool f64 )
     {
+        uint32_t lo = 0, hi = 0;
+        shard_range( n, opt, lo, hi );
+        const size_t rows = std::max<size_t>( hi - lo, 1 );
         const size_t nodes     = 2 * size_t( n ) - 1;
         const size_t sortBytes = sort_scratch_bytes( n );
         const size_t scanWords = output_scan_scratch_words( n );
@@ -350,7 +363,7 @@ namespace
                  + align256( 4 * nodes ) + align256( 4 * size_t( n ) ) + align256( sizeof( WideNode ) * n );
         total += align256( sortBytes );
         total += align256( size_t( n ) ) + align256( 4 * size_t( n ) * opt.k ) + align256( 4 * size_t( n ) ) * 3
-                 + align256( sizeof( uint4 ) * kMaxVertices * size_t( n ) ) + align256( sizeof( uint4 ) * kMaxEdges * size_t( n ) );
+                 + align256( sizeof( uint4 ) * kMaxVertices * rows ) + align256( sizeof( uint4 ) * kMaxEdges * rows );
         total += align256( 4 * size_t( n ) ) + align256( 4 * 64 ) + align256( 4 );
         total += align256( 4 * size_t( n ) ) * 2 + align256( 4 * scanWords * 2 ) + align256( 16 );
         total += align256( spec_bytes( n ) );
@@ -391,8 +404,8 @@ namespace
         CellContext & c   = h->cells;
         c.n               = n;
         c.k               = opt.k;
-        c.lo              = uint32_t( uint64_t( n ) * opt.shard_index / opt.shard_count );
-        c.hi              = uint32_t( uint64_t( n ) * ( opt.shard_index + 1 ) / opt.shard_count );
+        shard_range( n, opt, c.lo, c.hi );
+        const size_t rows = std::max<size_t>( c.hi - c.lo, 1 );
         c.sites           = t.sites;
         c.sites_f         = t.sites_f;
         c.nodes           = t.nodes;
@@ -402,8 +415,8 @@ namespace
         c.known_radii     = a.take<float>( n );
         c.vertex_nb       = a.take<uint32_t>( n );
         c.edge_nb         = a.take<uint32_t>( n );
-        c.vertices        = a.take<uint4>( size_t( n ) * kMaxVertices );
-        c.edges           = a.take<uint4>( size_t( n ) * kMaxEdges );
+        c.vertices        = a.take<uint4>( rows * kMaxVertices ); // rows of cells [lo, hi)
+        c.edges           = a.take<uint4>( rows * kMaxEdges );
         h->tasks          = a.take<uint32_t>( n );
         h->task_counts    = a.take<uint32_t>( 64 );
         h->error          = a.take<uint32_t>( 1 );
@@ -633,8 +646,9 @@ namespace
     const uint32_t n        = h->n;
     const auto     vnb      = download( h->cells.vertex_nb, n );
     const auto     enb      = download( h->cells.edge_nb, n );
-    const auto     vertices = download( h->cells.vertices, size_t( n ) * kMaxVertices );
-    const auto     edges    = download( h->cells.edges, size_t( n ) * kMaxEdges );
+    const CellContext & c   = h->cells;
+    const auto     vertices = download( c.vertices, size_t( c.hi - c.lo ) * kMaxVertices );
+    const auto     edges    = download( c.edges, size_t( c.hi - c.lo ) * kMaxEdges );
     const auto     ix       = download( h->tree.indices, n );
     std::vector<std::pair<uint32_t, uint32_t>> bis;
     std::vector<std::tuple<uint32_t, uint32_t>> tris;
@@ -646,7 +660,7 @@ namespace
         quads.clear();
         for ( uint32_t e = 0; e < std::min( enb[ i ], kMaxEdges ); e++ )
         {
-            const uint4 r = edges[ size_t( i ) * kMaxEdges + e ];
+            const uint4 r = edges[ store_row( c, i ) * kMaxEdges + e ];
             if ( i < r.x && r.x < n )
                 bis.emplace_back( i, r.x );
             if ( i < r.y && r.y < n )
@@ -656,7 +670,7 @@ namespace
         }
         for ( uint32_t v = 0; v < std::min( vnb[ i ], kMaxVertices ); v++ )
         {
-            const uint4 r = vertices[ size_t( i ) * kMaxVertices + v ];
+            const uint4 r = vertices[ store_row( c, i ) * kMaxVertices + v ];
             if ( i < r.x && i < r.y && i < r.z && r.x < n && r.y < n && r.z < n )
                 quads.emplace_back( r.x, r.y, r.z );
         }
@@ -1030,8 +1044,8 @@ apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, 
     cudaMemcpy( &en, h->cells.edge_nb + sorted, 4, cudaMemcpyDeviceToHost );
     vn            = std::min( vn, kMaxVertices );
     en            = std::min( en, kMaxEdges );
-    const auto vr = download( h->cells.vertices + size_t( sorted ) * kMaxVertices, vn );
-    const auto er = download( h->cells.edges + size_t( sorted ) * kMaxEdges, en );
+    const auto vr = download( h->cells.vertices + store_row( h->cells, sorted ) * kMaxVertices, vn );
+    const auto er = download( h->cells.edges + store_row( h->cells, sorted ) * kMaxEdges, en );
     auto       map = [ & ]( uint32_t id ) { return id < h->n ? ix[ id ] : id; };
     if ( vcount )
         *vcount = vn;
@@ -1097,11 +1111,12 @@ apo2_status apo2_debug_array( apo2_handle * h, const char * name, void * dst, ui
         const bool  isV  = key == "vertices";
         const auto  nb   = download( isV ? h->cells.vertex_nb : h->cells.edge_nb, n );
         const uint32_t cap = isV ? kMaxVertices : kMaxEdges;
-        const auto  all  = download( isV ? h->cells.vertices : h->cells.edges, size_t( n ) * cap );
-        for ( uint32_t i = 0; i < n; i++ )
+        const CellContext & c = h->cells;
+        const auto  all  = download( isV ? c.vertices : c.edges, size_t( c.hi - c.lo ) * cap );
+        for ( uint32_t i = c.lo; i < c.hi; i++ ) // the stores hold this shard's cells
             for ( uint32_t r = 0; r < std::min( nb[ i ], cap ); r++ )
             {
-                const uint4 x = all[ size_t( i ) * cap + r ];
+                const uint4 x = all[ store_row( c, i ) * cap + r ];
                 packed.insert( packed.end(), { x.x, x.y, x.z, x.w } );
             }
         elems = packed.size();

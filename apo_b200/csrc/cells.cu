@@ -608,14 +608,14 @@ namespace apo2
     {
         w.en = c.edge_nb[ i ];
         for ( uint32_t e = lane_id(); e < w.en; e += 32 )
-            w.e[ e ] = c.edges[ size_t( i ) * kMaxEdges + e ];
+            w.e[ e ] = c.edges[ store_row( c, i ) * kMaxEdges + e ];
         w.vn = 0;
         if ( with_vertices )
         {
             w.vn = c.vertex_nb[ i ];
             for ( uint32_t v = lane_id(); v < w.vn; v += 32 )
             {
-                const uint4 r = c.vertices[ size_t( i ) * kMaxVertices + v ];
+                const uint4 r = c.vertices[ store_row( c, i ) * kMaxVertices + v ];
                 w.v[ v ]      = r;
                 if ( solve )
                     w.pos[ v ] = solve_vertex( c, si, r );
@@ -634,9 +634,9 @@ namespace apo2
         if ( w.en > kMaxEdges )
             err |= kErrEdgeCap;
         for ( uint32_t e = lane_id(); e < en; e += 32 )
-            c.edges[ size_t( i ) * kMaxEdges + e ] = w.e[ e ];
+            c.edges[ store_row( c, i ) * kMaxEdges + e ] = w.e[ e ];
         for ( uint32_t v = lane_id(); v + vertex_base < vn; v += 32 )
-            c.vertices[ size_t( i ) * kMaxVertices + vertex_base + v ] = w.v[ v ];
+            c.vertices[ store_row( c, i ) * kMaxVertices + vertex_base + v ] = w.v[ v ];
         if ( lane_id() == 0 )
         {
             c.vertex_nb[ i ] = vn;
@@ -1466,7 +1466,7 @@ namespace apo2
                     const uint32_t svn  = c.vertex_nb[ i ];
                     for ( uint32_t v = 0; v < svn; v++ )
                     {
-                        const uint4 r = c.vertices[ size_t( i ) * kMaxVertices + v ];
+                        const uint4 r = c.vertices[ store_row( c, i ) * kMaxVertices + v ];
                         if ( vertex_on_edge( r, k, l ) )
                             wmax = fmax( wmax, solve_vertex( c, si, r ).w );
                     }
@@ -1501,7 +1501,7 @@ namespace apo2
                     // the edge's index in the stored cell, where the proof's bits refer
                     for ( uint32_t e0 = 0; e0 < stored_en; e0++ )
                     {
-                        const uint4 r0 = c.edges[ size_t( i ) * kMaxEdges + e0 ];
+                        const uint4 r0 = c.edges[ store_row( c, i ) * kMaxEdges + e0 ];
                         if ( r0.x == k && r0.y == l )
                         {
                             skip = !( ( maybe[ e0 >> 5 ] >> ( e0 & 31 ) ) & 1u );
@@ -2005,9 +2005,9 @@ namespace apo2
             {
                 const uint32_t vn = c.vertex_nb[ i ], en = c.edge_nb[ i ];
                 for ( uint32_t v = lane; v < vn; v += 32 )
-                    vc += owns_vertex( i, c.vertices[ size_t( i ) * kMaxVertices + v ], c.n ) ? 1u : 0u;
+                    vc += owns_vertex( i, c.vertices[ store_row( c, i ) * kMaxVertices + v ], c.n ) ? 1u : 0u;
                 for ( uint32_t e = lane; e < en; e += 32 )
-                    cc += owns_closed( i, c.edges[ size_t( i ) * kMaxEdges + e ], c.n ) ? 1u : 0u;
+                    cc += owns_closed( i, c.edges[ store_row( c, i ) * kMaxEdges + e ], c.n ) ? 1u : 0u;
             }
             vc = __reduce_add_sync( kFull, vc );
             cc = __reduce_add_sync( kFull, cc );
@@ -2041,7 +2041,7 @@ namespace apo2
                 bool           own = false;
                 if ( v < vn )
                 {
-                    r   = c.vertices[ size_t( i ) * kMaxVertices + v ];
+                    r   = c.vertices[ store_row( c, i ) * kMaxVertices + v ];
                     own = owns_vertex( i, r, c.n );
                 }
                 const uint32_t bal = __ballot_sync( kFull, own );
@@ -2061,7 +2061,7 @@ namespace apo2
                 bool           own = false;
                 if ( e < en )
                 {
-                    r   = c.edges[ size_t( i ) * kMaxEdges + e ];
+                    r   = c.edges[ store_row( c, i ) * kMaxEdges + e ];
                     own = owns_closed( i, r, c.n );
                 }
                 const uint32_t bal = __ballot_sync( kFull, own );

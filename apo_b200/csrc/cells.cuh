@@ -44,6 +44,10 @@ namespace apo2
         uint32_t *       work_counter = nullptr; // next cell of the dynamically scheduled passes
     };
 
+    // Row of cell i in the per-cell stores (vertices, edges), which hold only the cells
+    // [lo, hi) a handle builds: a shard of the diagram needs stores for its own cells alone.
+    __host__ __device__ __forceinline__ size_t store_row( const CellContext & c, uint32_t i ) { return size_t( i - c.lo ); }
+
     // Exact edge validation: a lane walks its edge's search alone for kLaneWalk steps; a
     // search still running then is finished by the whole warp, in the same order, from a
     // frontier of at most kCoopCap nodes kept in global scratch (plus each lane's saved stack),

@@ -81,7 +81,7 @@ namespace apo2
                 uint32_t v = kNone;
                 if ( x < total )
                 {
-                    const uint4 r = c.edges[ size_t( i ) * kMaxEdges + ( x >> 1 ) ];
+                    const uint4 r = c.edges[ store_row( c, i ) * kMaxEdges + ( x >> 1 ) ];
                     v             = ( x & 1 ) ? r.y : r.x;
                 }
                 ids[ x ] = v;
@@ -206,7 +206,7 @@ namespace apo2
         const uint32_t vn   = c.vertex_nb[ s.i ];
         for ( uint32_t v = 0; v < vn; v++ )
         {
-            const uint4 r = c.vertices[ size_t( s.i ) * kMaxVertices + v ];
+            const uint4 r = c.vertices[ store_row( c, s.i ) * kMaxVertices + v ];
             if ( vertex_on_edge( r, s.k, s.l ) )
                 wmax = fmax( wmax, solve_vertex( c, s.si, r ).w );
         }
@@ -341,7 +341,7 @@ namespace apo2
                         else
                         {
                             s.i           = tasks[ s.t ];
-                            const uint4 r = c.edges[ size_t( s.i ) * kMaxEdges + e ];
+                            const uint4 r = c.edges[ store_row( c, s.i ) * kMaxEdges + e ];
                             s.k           = r.x;
                             s.l           = r.y;
                             s.closed      = r.z == kNone;
@@ -495,7 +495,7 @@ namespace apo2
         s.t           = h.x;
         s.e           = h.y;
         s.i           = tasks[ s.t ];
-        const uint4 r = c.edges[ size_t( s.i ) * kMaxEdges + s.e ];
+        const uint4 r = c.edges[ store_row( c, s.i ) * kMaxEdges + s.e ];
         s.k           = r.x;
         s.l           = r.y;
         s.closed      = r.z == kNone;
@@ -633,7 +633,7 @@ namespace apo2
             const uint32_t en = c.edge_nb[ i ];
             for ( uint32_t e = lane; e < en; e += 32 )
             {
-                uint32_t * w = &c.edges[ size_t( i ) * kMaxEdges + e ].w;
+                uint32_t * w = &c.edges[ store_row( c, i ) * kMaxEdges + e ].w;
                 *w           = ( *w & 0xffffff00u ) | 1u;
             }
             if ( lane == 0 )

@@ -37,6 +37,8 @@ def test_shards_concatenate_to_the_whole_diagram(case, count):
     assert sum(p[2]["buried"] for p in parts) == stats["buried"]
     assert sum(p[2]["vertex_records"] for p in parts) == stats["vertex_records"]
     assert all(p[2]["error_flags"] == 0 for p in parts)
+    # a shard holds per-cell stores for its own cells only
+    assert all(p[2]["device_bytes"] < stats["device_bytes"] for p in parts)
 
 
 def test_shards_with_other_k_and_knn_steps():
