@@ -114,6 +114,7 @@ COMPAT_PROGRAM = r"""
 #include <cstdio>
 #include <vector>
 #include "apo/gpu/algorithm.hpp"
+#include "apo/gpu/cavity.hpp"
 
 // instantiate the whole mirror so every member is type-checked against the C ABI
 template class apo::gpu::AlgorithmGPU<16>;
@@ -126,7 +127,15 @@ int main(int argc, char **) {
     std::vector<apo::Real> sites(xyzr.begin(), xyzr.end());
     apo::ConstSpan<apo::Real> span{sites};
     if (span.size != sites.size()) return 2;
+    // the cavity application's directions are computed on the host
+    const std::vector<float> dirs = apo::gpu::getDirections(64);
+    if (dirs.size() != 192 || dirs[0] != 0.f || dirs[1] != 0.f || dirs[2] != -1.f) return 3;
     if (argc > 5) {  // never taken in the test: shows the reference's call sequence compiles
+        apo::gpu::CavityDetection cavity{span};
+        std::vector<float> loaded(xyzr.begin(), xyzr.end());
+        auto ratios = cavity.getHitRatios(apo::ConstSpan<float>{loaded});
+        auto found = cavity.filterVertices({cavity.vertexNb(), .5f, 5.f});
+        std::printf("%zu %zu\n", ratios.size(), found.size());
         apo::gpu::AlgorithmGPU<16> algo{span};
         algo.build();
         auto full = algo.toHostFull(true);
