@@ -47,7 +47,7 @@ class Options(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("k", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32),
                 ("device", ctypes.c_uint32), ("stage_timing", ctypes.c_uint32), ("edge_search", ctypes.c_uint32),
                 ("knn_steps", ctypes.c_uint32), ("stop_after", ctypes.c_uint32), ("shard_index", ctypes.c_uint32),
-                ("shard_count", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
+                ("shard_count", ctypes.c_uint32), ("wait_limit", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 5)]
 
 
 class Stats(ctypes.Structure):
@@ -58,7 +58,8 @@ class Stats(ctypes.Structure):
                 ("ms_bounds", ctypes.c_double), ("ms_sort", ctypes.c_double), ("ms_tree", ctypes.c_double),
                 ("ms_knn", ctypes.c_double), ("ms_cells", ctypes.c_double), ("ms_vertex_validation", ctypes.c_double),
                 ("ms_edge_validation", ctypes.c_double), ("ms_bisector_validation", ctypes.c_double),
-                ("ms_output", ctypes.c_double), ("device_bytes", ctypes.c_uint64)]
+                ("ms_output", ctypes.c_double), ("device_bytes", ctypes.c_uint64), ("uncertified", ctypes.c_uint32),
+                ("reserved32", ctypes.c_uint32)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("reserved")}
@@ -97,6 +98,7 @@ SIGNATURES = {
     "apo2_topology_json": (_I, [_P, _P, _U64, _P]),
     "apo2_certify": (_I, [_P, _P, _P, _U64, _U32, _I, _P, _P]),
     "apo2_contribution_profile": (_I, [_P, _U32, _P, _P]),
+    "apo2_vertex_error": (_I, [_P, _P, _P, _U64, _I, ctypes.c_double, _P, _P, _P, _P]),
     "apo2_batch_create": (_I, [_U32, _U32, _P, _P]),
     "apo2_batch_build": (_I, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "apo2_batch_destroy": (_I, [_P]),
@@ -169,10 +171,12 @@ class AlgorithmGPU:
     """Counterpart of `apo::gpu::AlgorithmGPU<K>` (algorithm.cuh:12-46)."""
 
     def __init__(self, sites, knnValidationStep: int = 1, k: int = 16, max_iterations: int = 10, device: int = 0,
-                 stage_timing: bool = False, edge_search: int = 0, stop_after: int = 0, shard: tuple[int, int] = (0, 1)):
+                 stage_timing: bool = False, edge_search: int = 0, stop_after: int = 0, shard: tuple[int, int] = (0, 1),
+                 wait_limit: int = 0):
         """`shard` = (index, count): build only the cells of one of `count` contiguous Morton
         ranges of the sites (one diagram over several GPUs); the shards' outputs, concatenated in
-        shard order, are the whole diagram's."""
+        shard order, are the whole diagram's. `wait_limit`: polls per look-back wait of the
+        LBVH's radix sort before a tile recounts its digits itself (0 = the library default)."""
         lib = load_library()
         self._sites, dtype = _as_sites(sites)
         self.n = int(self._sites.shape[0])
@@ -186,6 +190,7 @@ class AlgorithmGPU:
         opt.knn_steps = APO2_NO_KNN_STEPS if knnValidationStep == 0 else knnValidationStep
         opt.stop_after = stop_after
         opt.shard_index, opt.shard_count = int(shard[0]), int(shard[1])
+        opt.wait_limit = int(wait_limit)
         self.knnValidationStep = knnValidationStep
         self._k = k
         handle = ctypes.c_void_p()
@@ -207,6 +212,9 @@ class AlgorithmGPU:
         return self._h
 
     def build(self, stream: int = 0, synchronize: bool = True) -> None:
+        """Builds the diagram. With `synchronize` the build's status is checked: Apo2Error with
+        APO2_ERR_CAPACITY or APO2_ERR_ITER_LIMIT still leaves the diagram readable, as the
+        reference leaves it."""
         _check(self._lib.apo2_build(self._h, ctypes.c_void_p(stream), 1 if synchronize else 0))
 
     def build_and_extract(self, stream: int = 0) -> None:
@@ -260,6 +268,24 @@ class AlgorithmGPU:
         _check(self._lib.apo2_certify(self._h, p.ctypes.data, i.ctypes.data, p.shape[0], arity, APO2_HOST,
                                       flags.ctypes.data, ctypes.byref(bad)))
         return bad.value, flags[:p.shape[0]]
+
+    def vertex_error(self, positions=None, ids=None, threshold: float = 1e-5):
+        """Per-result error of output vertices against Newton-refined IEEE double solves of
+        their four sites (the handle's last output when positions is None). Returns
+        (max error, count above threshold, singular count, per-vertex errors float32)."""
+        mx, above, singular = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_uint64()
+        if positions is None:
+            count = self.output_counts()[0]
+            errs = np.zeros(max(count, 1), dtype=np.float32)
+            _check(self._lib.apo2_vertex_error(self._h, None, None, 0, APO2_HOST, threshold, errs.ctypes.data,
+                                               ctypes.byref(mx), ctypes.byref(above), ctypes.byref(singular)))
+            return mx.value, above.value, singular.value, errs[:count]
+        p = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 4))
+        i = np.ascontiguousarray(np.asarray(ids, dtype=np.uint32).reshape(-1, 4))
+        errs = np.zeros(max(p.shape[0], 1), dtype=np.float32)
+        _check(self._lib.apo2_vertex_error(self._h, p.ctypes.data, i.ctypes.data, p.shape[0], APO2_HOST, threshold,
+                                           errs.ctypes.data, ctypes.byref(mx), ctypes.byref(above), ctypes.byref(singular)))
+        return mx.value, above.value, singular.value, errs[:p.shape[0]]
 
     def contribution_profile(self, steps: int = 4):
         """Per-rank labels of the kNN cell construction (sorted cell order): (contributed,

@@ -60,7 +60,12 @@ namespace
         }
     };
 
-    constexpr int kStages = 10;
+    constexpr int      kStages    = 10;
+    constexpr uint32_t kMaxRounds = 64; // validation rounds at most (apo2_options.max_iterations)
+
+    // Error-word flags that mean the per-cell stores could not hold a cell (the results of
+    // those cells are incomplete), and those that mean a bounded loop stopped early.
+    constexpr uint32_t kCapacityFlags = kErrVertexCap | kErrEdgeCap | kErrNewEdgeCap | kErrBisector | kErrStack;
 } // namespace
 
 struct apo2_handle
@@ -213,7 +218,7 @@ namespace
         launch_bounds( h->input, h->input_f64, n, h->input_d4, h->partials, h->partial_count, h->bounds_counter, h->scene,
                        h->tree.sites + n, s );
         record( h, 1, s );
-        launch_tree( h->tree, n, h->input_d4, h->scene, h->sort, s );
+        launch_tree( h->tree, n, h->input_d4, h->scene, h->sort, s, h->options.wait_limit );
         record( h, 2, s ); // bounds+Morton+sort+tree recorded as one span plus the sort below
         // kNN steps (algorithm.inl:1535-1549); with several, the kNN span is the first
         // step's search and the cells span everything after it
@@ -237,7 +242,7 @@ namespace
         const uint32_t stop   = h->options.stop_after;
         bool           halted = stop == 1;
         const uint32_t rounds = h->options.max_iterations;
-        cudaMemsetAsync( h->task_counts, 0, sizeof( uint32_t ) * rounds, s );
+        cudaMemsetAsync( h->task_counts, 0, sizeof( uint32_t ) * ( rounds + 1 ), s );
         for ( uint32_t r = 0; r < rounds && !halted; r++ )
         {
             launch_tasks( h->cells, h->tasks, h->task_counts + r, s );
@@ -250,6 +255,9 @@ namespace
                 launch_edge_validation_speculative( h->cells, h->tasks, h->task_counts + r, h->spec, s );
             halted = stop == 3 + 2 * r;
         }
+        // cells still in validation after the last round (the reference leaves them as they are)
+        if ( stop == 0 )
+            launch_tasks( h->cells, h->tasks, h->task_counts + rounds, s );
         record( h, 5, s );
         if ( stop == 0 )
             launch_bisector_validation( h->cells, s );
@@ -276,15 +284,33 @@ namespace
         return APO2_OK;
     }
 
+    // Error status of a finished build: per-cell store overflows first, then cells that were
+    // still uncertified after the last validation round, or a bounded walk or restart loop
+    // that stopped early. The diagram is complete either way, as the reference leaves it.
+    apo2_status build_status( apo2_handle * h, uint32_t err, uint32_t uncertified )
+    {
+        h->stats.error_flags = err;
+        h->stats.uncertified = uncertified;
+        if ( err & kCapacityFlags )
+            return fail( APO2_ERR_CAPACITY, "capacity flags " + std::to_string( err ) );
+        if ( uncertified )
+            return fail( APO2_ERR_ITER_LIMIT, std::to_string( uncertified ) + " cells still uncertified after " +
+                                                  std::to_string( h->options.max_iterations ) + " validation rounds" );
+        if ( err & kErrWalk )
+            return fail( APO2_ERR_ITER_LIMIT, "a traversal or restart loop reached its bound" );
+        return APO2_OK; // kErrSortSpin alone: a look-back wait ran out and its recount kept the order exact
+    }
+
     apo2_status finish( apo2_handle * h, cudaStream_t s )
     {
         APO2_CUDA( cudaStreamSynchronize( s ), "build" );
-        uint32_t err = 0;
+        uint32_t err = 0, uncertified = 0;
         APO2_CUDA( cudaMemcpy( &err, h->error, sizeof( uint32_t ), cudaMemcpyDeviceToHost ), "error word" );
-        h->stats.error_flags = err;
-        if ( err )
-            return fail( APO2_ERR_CAPACITY, "capacity flags " + std::to_string( err ) );
-        return APO2_OK;
+        if ( h->options.stop_after == 0 )
+            APO2_CUDA( cudaMemcpy( &uncertified, h->task_counts + h->options.max_iterations, sizeof( uint32_t ),
+                                   cudaMemcpyDeviceToHost ),
+                       "uncertified count" );
+        return build_status( h, err, uncertified );
     }
 
     // Makes sure the output arrays hold everything the last extraction counted (one
@@ -364,7 +390,7 @@ namespace
         total += align256( sortBytes );
         total += align256( size_t( n ) ) + align256( 4 * size_t( n ) * opt.k ) + align256( 4 * size_t( n ) ) * 3
                  + align256( sizeof( uint4 ) * kMaxVertices * rows ) + align256( sizeof( uint4 ) * kMaxEdges * rows );
-        total += align256( 4 * size_t( n ) ) + align256( 4 * 64 ) + align256( 4 );
+        total += align256( 4 * size_t( n ) ) + align256( 4 * ( kMaxRounds + 1 ) ) + align256( 4 );
         total += align256( 4 * size_t( n ) ) * 2 + align256( 4 * scanWords * 2 ) + align256( 16 );
         total += align256( spec_bytes( n ) );
         total += align256( walk_scratch_bytes() ) + align256( 4 );
@@ -418,7 +444,7 @@ namespace
         c.vertices        = a.take<uint4>( rows * kMaxVertices ); // rows of cells [lo, hi)
         c.edges           = a.take<uint4>( rows * kMaxEdges );
         h->tasks          = a.take<uint32_t>( n );
-        h->task_counts    = a.take<uint32_t>( 64 );
+        h->task_counts    = a.take<uint32_t>( kMaxRounds + 1 );
         h->error          = a.take<uint32_t>( 1 );
         c.error           = h->error;
         c.scene           = h->scene;
@@ -460,7 +486,7 @@ namespace
             opt.knn_steps = 0;
         else if ( opt.knn_steps > 64 )
             return fail( APO2_ERR_INVALID_ARG, "knn_steps is at most 64" );
-        opt.max_iterations = std::min( opt.max_iterations, 64u );
+        opt.max_iterations = std::min( opt.max_iterations, kMaxRounds );
         if ( opt.shard_count == 0 )
             opt.shard_count = 1;
         if ( opt.shard_index >= opt.shard_count )
@@ -839,6 +865,81 @@ apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint3
     return APO2_OK;
 }
 
+apo2_status apo2_vertex_error( apo2_handle * h, const double * positions, const uint32_t * ids, uint64_t count,
+                               apo2_location location, double threshold, float * errors, double * max_error, uint64_t * above,
+                               uint64_t * singular )
+{
+    if ( !h || !max_error || ( ( positions == nullptr ) != ( ids == nullptr ) )
+         || ( location != APO2_HOST && location != APO2_DEVICE ) || !( threshold >= 0.0 ) )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_vertex_error" );
+    if ( !h->built )
+        return fail( APO2_ERR_NOT_BUILT, "no build yet" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    const double4 * P = nullptr;
+    const uint4 *   I = nullptr;
+    if ( !positions )
+    {
+        apo2_status st = settle_output( h, 0 );
+        if ( st != APO2_OK )
+            return st;
+        count = h->stats.output_vertices;
+        P     = h->out.vpos;
+        I     = h->out.vids;
+    }
+    const size_t err_bytes = errors ? align256( sizeof( float ) * std::max<uint64_t>( count, 1 ) ) : 0;
+    const size_t in_bytes  = positions && location == APO2_HOST ? align256( sizeof( double4 ) * count ) + align256( sizeof( uint4 ) * count ) : 0;
+    void *       scratch   = nullptr;
+    APO2_CUDA( cudaMalloc( &scratch, 256 + err_bytes + in_bytes ), "vertex error scratch" );
+    char *               base   = static_cast<char *>( scratch );
+    unsigned long long * counts = reinterpret_cast<unsigned long long *>( base ); // max bits, above, singular
+    float *              derr   = errors ? reinterpret_cast<float *>( base + 256 ) : nullptr;
+    cudaError_t          e      = cudaSuccess;
+    if ( positions )
+    {
+        if ( location == APO2_HOST )
+        {
+            double4 * dp = reinterpret_cast<double4 *>( base + 256 + err_bytes );
+            uint4 *   di = reinterpret_cast<uint4 *>( base + 256 + err_bytes + align256( sizeof( double4 ) * count ) );
+            e            = cudaMemcpy( dp, positions, sizeof( double4 ) * count, cudaMemcpyHostToDevice );
+            if ( e == cudaSuccess )
+                e = cudaMemcpy( di, ids, sizeof( uint4 ) * count, cudaMemcpyHostToDevice );
+            P = dp;
+            I = di;
+        }
+        else
+        {
+            P = reinterpret_cast<const double4 *>( positions );
+            I = reinterpret_cast<const uint4 *>( ids );
+        }
+    }
+    if ( e == cudaSuccess )
+        e = cudaMemset( counts, 0, 3 * sizeof( unsigned long long ) );
+    if ( e == cudaSuccess && count )
+    {
+        ObserveScope observe( h );
+        launch_vertex_error( h->input_d4, h->n, P, I, count, threshold, derr, counts, counts + 1, counts + 2, 0 );
+        e = cudaGetLastError();
+    }
+    unsigned long long host[ 3 ] = {};
+    if ( e == cudaSuccess )
+        e = cudaDeviceSynchronize();
+    if ( e == cudaSuccess )
+        e = cudaMemcpy( host, counts, sizeof( host ), cudaMemcpyDeviceToHost );
+    if ( e == cudaSuccess && errors && count )
+        e = cudaMemcpy( errors, derr, sizeof( float ) * count, cudaMemcpyDeviceToHost );
+    cudaFree( scratch );
+    if ( e != cudaSuccess )
+        return cuda_fail( e, "vertex error" );
+    double mx = 0.0;
+    std::memcpy( &mx, &host[ 0 ], sizeof( mx ) );
+    *max_error = mx;
+    if ( above )
+        *above = host[ 1 ];
+    if ( singular )
+        *singular = host[ 2 ];
+    return APO2_OK;
+}
+
 apo2_status apo2_cavity_directions( uint32_t count, float * xyz )
 {
     if ( !xyz || count == 0 || count > kCavityMaxSamples )
@@ -1000,7 +1101,7 @@ apo2_status apo2_contribution_profile( apo2_handle * h, uint32_t steps, uint8_t 
         cudaMemsetAsync( h->error, 0, sizeof( uint32_t ), s );
         launch_bounds( h->input, h->input_f64, n, h->input_d4, h->partials, h->partial_count, h->bounds_counter, h->scene,
                        h->tree.sites + n, s );
-        launch_tree( h->tree, n, h->input_d4, h->scene, h->sort, s );
+        launch_tree( h->tree, n, h->input_d4, h->scene, h->sort, s, h->options.wait_limit );
         for ( uint32_t step = 0; step < steps; step++ )
         {
             launch_knn( h->cells, step, s );
@@ -1147,8 +1248,8 @@ apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
     const auto     enb    = download( h->cells.edge_nb, n );
     uint32_t       err    = 0;
     cudaMemcpy( &err, h->error, 4, cudaMemcpyDeviceToHost );
-    uint32_t counts[ 64 ] = {};
-    cudaMemcpy( counts, h->task_counts, 4 * h->options.max_iterations, cudaMemcpyDeviceToHost );
+    uint32_t counts[ kMaxRounds + 1 ] = {};
+    cudaMemcpy( counts, h->task_counts, 4 * ( h->options.max_iterations + 1 ), cudaMemcpyDeviceToHost );
     apo2_stats s = h->stats;
     s.n          = n;
     s.buried = 0;
@@ -1165,6 +1266,7 @@ apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
     for ( uint32_t r = 0; r < h->options.max_iterations; r++ )
         s.validation_rounds += counts[ r ] != 0;
     s.error_flags     = err;
+    s.uncertified     = h->options.stop_after == 0 ? counts[ h->options.max_iterations ] : 0;
     s.kernel_launches = h->launches;
     if ( h->timing )
     {

@@ -2187,35 +2187,57 @@ namespace apo2
     // -----------------------------------------------------------------------------------
     // Launch helpers
     // -----------------------------------------------------------------------------------
-    static int g_cell_grid = 0;
+    // Kernel attributes (dynamic shared memory above 48 KB) are per device, and so is the
+    // persistent grid size derived from the device's SM count: both are set up once per
+    // device, on the device current at the launch.
+    constexpr int       kGridDevices = 64;
+    static int          g_cell_grid[ kGridDevices ] = {};
+    static PerDeviceOnce g_cell_config;
+
+    static int current_device()
+    {
+        int dev = 0;
+        cudaGetDevice( &dev );
+        return dev;
+    }
+
+    static int & cell_grid_slot()
+    {
+        static int fallback = 0;
+        const int  dev      = current_device();
+        return ( dev >= 0 && dev < kGridDevices ) ? g_cell_grid[ dev ] : fallback;
+    }
 
     void configure_cell_kernels()
     {
-        if ( g_cell_grid )
-            return;
-        int dev = 0, sms = 148;
-        cudaGetDevice( &dev );
-        cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
-        cudaFuncSetAttribute( k_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( false ) ) );
-        cudaFuncSetAttribute( k_vertex_validation, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( false ) ) );
-        cudaFuncSetAttribute( k_edge_validation, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( false ) ) );
-        cudaFuncSetAttribute( k_bisector_validation, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( true ) ) );
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_cells, kCellBlock, cell_smem_bytes( false ) );
-        g_cell_grid = sms * std::max( 1, per_sm );
+        g_cell_config.run( [] {
+            const int dev = current_device();
+            int       sms = 148;
+            cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
+            cudaFuncSetAttribute( k_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( false ) ) );
+            cudaFuncSetAttribute( k_cells_profile, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( false ) ) );
+            cudaFuncSetAttribute( k_vertex_validation, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( false ) ) );
+            cudaFuncSetAttribute( k_edge_validation, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( false ) ) );
+            cudaFuncSetAttribute( k_bisector_validation, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( true ) ) );
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_cells, kCellBlock, cell_smem_bytes( false ) );
+            cell_grid_slot() = sms * std::max( 1, per_sm );
+        } );
+        if ( cell_grid_slot() == 0 ) // an ordinal outside the table: size it for 148 SMs x 4 blocks
+            cell_grid_slot() = 148 * 4;
     }
 
     size_t walk_scratch_bytes()
     {
         configure_cell_kernels();
-        return size_t( g_cell_grid ) * ( kCellBlock / 32 ) * kWalkScratchWords * sizeof( uint32_t );
+        return size_t( cell_grid_slot() ) * ( kCellBlock / 32 ) * kWalkScratchWords * sizeof( uint32_t );
     }
 
     static int cell_grid( uint32_t cells )
     {
         configure_cell_kernels();
         const int needed = int( ( uint64_t( cells ) + ( kCellBlock / 32 ) - 1 ) / ( kCellBlock / 32 ) );
-        return std::max( 1, std::min( g_cell_grid, needed ) );
+        return std::max( 1, std::min( cell_grid_slot(), needed ) );
     }
 
     void launch_knn( const CellContext & c, uint32_t step, cudaStream_t s )
@@ -2233,12 +2255,6 @@ namespace apo2
                                cudaStream_t s )
     {
         configure_cell_kernels();
-        static bool configured = false;
-        if ( !configured )
-        {
-            cudaFuncSetAttribute( k_cells_profile, cudaFuncAttributeMaxDynamicSharedMemorySize, int( cell_smem_bytes( false ) ) );
-            configured = true;
-        }
         cudaMemsetAsync( c.work_counter, 0, sizeof( uint32_t ), s );
         APO2_LAUNCH( "k_cells_profile", s,
                      k_cells_profile<<<cell_grid( c.n ), kCellBlock, cell_smem_bytes( false ), s>>>( c, step, row, contributed, certified ) );

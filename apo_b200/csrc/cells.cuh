@@ -182,6 +182,12 @@ namespace apo2
     void launch_certify( const double4 * by_id, const double4 * sorted, const uint32_t * indices, const WideNode * nodes,
                          uint32_t n, const double4 * points, const uint4 * ids, uint32_t arity, uint64_t count, float rmax,
                          uint8_t * flags, unsigned long long * bad, uint32_t * error, cudaStream_t s );
+    // relative error of output vertices against Newton-refined IEEE double solves (certify.cu):
+    // per-vertex errors (optional), the largest (as the bits of a non-negative double), the
+    // count above `threshold` and the count of singular systems
+    void launch_vertex_error( const double4 * by_id, uint32_t n, const double4 * points, const uint4 * ids, uint64_t count,
+                              double threshold, float * errors, unsigned long long * max_bits, unsigned long long * above,
+                              unsigned long long * singular, cudaStream_t s );
     // grid sizes of the speculation kernels (once per process; call before concurrent builds)
     void configure_spec_kernels();
     void   spec_carve( SpecBuffers & b, void * base, uint32_t n );

@@ -150,6 +150,132 @@ namespace apo2
         }
     } // namespace
 
+    namespace
+    {
+        // Relative error of output vertices against an FP64 re-solve (the per-result error the
+        // build reports). The reference solves a vertex in double precision but takes every
+        // length with a single-precision square root (its `length`, gpu/math.cuh:307-309); the
+        // check here refines the stored vertex (x, y, z, w) with Newton steps on the four
+        // equations |p - c_a| - r_a - w = 0 of its sites, in IEEE double (correctly rounded
+        // square roots, 4x4 solves with partial pivoting), and reports
+        //     max over x, y, z, w of |stored - refined| / max(1, |refined|)
+        // (the measure of the parity tests). A vertex whose system is singular keeps its
+        // stored value as the refined one (error 0) and is counted in `singular`.
+        __device__ bool solve4( double a[ 4 ][ 5 ] )
+        {
+            for ( int c = 0; c < 4; c++ )
+            {
+                int    piv  = c;
+                double best = fabs( a[ c ][ c ] );
+                for ( int r = c + 1; r < 4; r++ )
+                    if ( fabs( a[ r ][ c ] ) > best )
+                    {
+                        best = fabs( a[ r ][ c ] );
+                        piv  = r;
+                    }
+                if ( !( best > 1e-300 ) )
+                    return false;
+                if ( piv != c )
+                    for ( int k = 0; k < 5; k++ )
+                    {
+                        const double t = a[ c ][ k ];
+                        a[ c ][ k ]    = a[ piv ][ k ];
+                        a[ piv ][ k ]  = t;
+                    }
+                for ( int r = c + 1; r < 4; r++ )
+                {
+                    const double f = a[ r ][ c ] / a[ c ][ c ];
+                    for ( int k = c; k < 5; k++ )
+                        a[ r ][ k ] = __fma_rn( -f, a[ c ][ k ], a[ r ][ k ] );
+                }
+            }
+            for ( int r = 3; r >= 0; r-- )
+            {
+                double v = a[ r ][ 4 ];
+                for ( int k = r + 1; k < 4; k++ )
+                    v = __fma_rn( -a[ r ][ k ], a[ k ][ 4 ], v );
+                a[ r ][ 4 ] = v / a[ r ][ r ];
+            }
+            return true;
+        }
+
+        __global__ void k_vertex_error( const double4 * __restrict__ by_id, uint32_t n, const double4 * __restrict__ points,
+                                        const uint4 * __restrict__ ids, uint64_t count, double threshold,
+                                        float * __restrict__ errors, unsigned long long * __restrict__ max_bits,
+                                        unsigned long long * __restrict__ above, unsigned long long * __restrict__ singular )
+        {
+            for ( uint64_t v = blockIdx.x * uint64_t( blockDim.x ) + threadIdx.x; v < count; v += uint64_t( gridDim.x ) * blockDim.x )
+            {
+                const double4  p0 = points[ v ];
+                const uint4    id = ids[ v ];
+                const uint32_t own[ 4 ] = { id.x, id.y, id.z, id.w };
+                double4        s[ 4 ];
+                bool           ok = true;
+                for ( int a = 0; a < 4; a++ )
+                {
+                    ok = ok && own[ a ] < n;
+                    s[ a ] = ok ? by_id[ own[ a ] ] : make_double4( 0, 0, 0, 0 );
+                }
+                double x[ 4 ] = { p0.x, p0.y, p0.z, p0.w };
+                for ( int it = 0; it < 4 && ok; it++ )
+                {
+                    double m[ 4 ][ 5 ];
+                    for ( int a = 0; a < 4; a++ )
+                    {
+                        const double dx = x[ 0 ] - s[ a ].x, dy = x[ 1 ] - s[ a ].y, dz = x[ 2 ] - s[ a ].z;
+                        const double d  = __dsqrt_rn( __fma_rn( dx, dx, __fma_rn( dy, dy, dz * dz ) ) );
+                        if ( !( d > 0.0 ) )
+                        {
+                            ok = false;
+                            break;
+                        }
+                        m[ a ][ 0 ] = dx / d;
+                        m[ a ][ 1 ] = dy / d;
+                        m[ a ][ 2 ] = dz / d;
+                        m[ a ][ 3 ] = -1.0;
+                        m[ a ][ 4 ] = -( d - s[ a ].w - x[ 3 ] );
+                    }
+                    if ( !ok || !solve4( m ) )
+                    {
+                        ok = false;
+                        break;
+                    }
+                    for ( int k = 0; k < 4; k++ )
+                        x[ k ] += m[ k ][ 4 ];
+                }
+                double err = 0.0;
+                if ( ok )
+                {
+                    const double got[ 4 ] = { p0.x, p0.y, p0.z, p0.w };
+                    for ( int k = 0; k < 4; k++ )
+                        err = fmax( err, fabs( got[ k ] - x[ k ] ) / fmax( 1.0, fabs( x[ k ] ) ) );
+                    if ( !( err == err ) ) // NaN: treat as singular
+                    {
+                        err = 0.0;
+                        ok  = false;
+                    }
+                }
+                if ( !ok )
+                    atomicAdd( singular, 1ull );
+                if ( errors )
+                    errors[ v ] = float( err );
+                if ( err > threshold )
+                    atomicAdd( above, 1ull );
+                atomicMax( max_bits, static_cast<unsigned long long>( __double_as_longlong( err ) ) );
+            }
+        }
+    } // namespace
+
+    void launch_vertex_error( const double4 * by_id, uint32_t n, const double4 * points, const uint4 * ids, uint64_t count,
+                              double threshold, float * errors, unsigned long long * max_bits, unsigned long long * above,
+                              unsigned long long * singular, cudaStream_t s )
+    {
+        const uint64_t blocks = std::min<uint64_t>( ( count + 255 ) / 256, 148 * 32 );
+        APO2_LAUNCH( "k_vertex_error", s,
+                     k_vertex_error<<<unsigned( std::max<uint64_t>( blocks, 1 ) ), 256, 0, s>>>( by_id, n, points, ids, count, threshold,
+                                                                                                errors, max_bits, above, singular ) );
+    }
+
     void launch_certify( const double4 * by_id, const double4 * sorted, const uint32_t * indices, const WideNode * nodes,
                          uint32_t n, const double4 * points, const uint4 * ids, uint32_t arity, uint64_t count, float rmax,
                          uint8_t * flags, unsigned long long * bad, uint32_t * error, cudaStream_t s )

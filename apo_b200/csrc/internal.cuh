@@ -6,6 +6,8 @@
 #include <cstdio>
 
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -41,6 +43,36 @@ namespace apo2
         if ( o.hook )
             o.hook( name, s, after, o.ctx );
     }
+
+    // Runs a set-up step (kernel attributes and the like) once per CUDA device, on the device
+    // current at the call; safe from several host threads.
+    class PerDeviceOnce
+    {
+      public:
+        template<class F>
+        void run( F && f )
+        {
+            int device = 0;
+            if ( cudaGetDevice( &device ) != cudaSuccess || device < 0 || device >= kDevices )
+            {
+                f(); // unknown ordinal: do it every time
+                return;
+            }
+            if ( done_[ device ].load( std::memory_order_acquire ) )
+                return;
+            std::lock_guard<std::mutex> lock( mutex_ );
+            if ( !done_[ device ].load( std::memory_order_relaxed ) )
+            {
+                f();
+                done_[ device ].store( true, std::memory_order_release );
+            }
+        }
+
+      private:
+        static constexpr int kDevices = 64;
+        std::atomic<bool>    done_[ kDevices ] = {};
+        std::mutex           mutex_;
+    };
 
     constexpr uint32_t kNone = 0xffffffffu;
 
@@ -114,7 +146,9 @@ namespace apo2
     };
     size_t sort_scratch_bytes( uint32_t n );
     void   sort_scratch_carve( SortScratch & s, void * base, uint32_t n, uint32_t * error_word );
-    void   radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t n, SortScratch & s, cudaStream_t stream );
+    // spin_limit: polls per look-back wait before the exact recount takes over (0 = default)
+    void   radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t n, SortScratch & s, cudaStream_t stream,
+                             uint32_t spin_limit = 0 );
 
     struct Tree
     {
@@ -136,7 +170,7 @@ namespace apo2
                           uint32_t partial_count, uint32_t * counter, Scene * scene, double4 * artificial, cudaStream_t s );
     size_t bounds_partial_bytes( uint32_t count );
     void   launch_tree( const Tree & t, uint32_t n, const double4 * input, const Scene * scene, SortScratch & sort,
-                        cudaStream_t s );
+                        cudaStream_t s, uint32_t spin_limit = 0 );
     void   launch_lbvh_f32( const float4 * sites, uint32_t n, float3 lo, float3 scale, uint32_t * indices, uint64_t * codes,
                             int32_t * parent, int32_t * left, int32_t * right, float4 * boxes, uint32_t * sizes,
                             uint32_t * arrivals, SortScratch & sort, cudaStream_t s );

@@ -413,10 +413,10 @@ namespace apo2
     size_t bounds_partial_bytes( uint32_t count ) { return sizeof( BoundsPartial ) * count; }
 
     void launch_tree( const Tree & t, uint32_t n, const double4 * input, const Scene * scene, SortScratch & sort,
-                      cudaStream_t s )
+                      cudaStream_t s, uint32_t spin_limit )
     {
         APO2_LAUNCH( "k_morton", s, k_morton<<<blocks_for( n, 256 ), 256, 0, s>>>( input, scene, n, t.codes, t.indices ) );
-        radix_sort_pairs( t.codes, t.indices, n, sort, s );
+        radix_sort_pairs( t.codes, t.indices, n, sort, s, spin_limit );
         APO2_LAUNCH( "k_leaves", s, k_leaves<<<blocks_for( n, 256 ), 256, 0, s>>>( input, t.indices, n, t.sites, t.sites_f, t.boxes, t.left, t.right ) );
         if ( n > 1 )
         {

@@ -9,8 +9,12 @@
 // order) and therefore the tie-break of the hierarchy.
 //
 // The look-back spins on flags published by blocks that started earlier (tile ids are
-// handed out by an atomic counter in start order), and every spin has an iteration limit
-// after which the kernel raises kErrSortSpin instead of waiting longer.
+// handed out by an atomic counter in start order, so every awaited tile is resident and
+// finishes its count without waiting). Every spin still has an iteration limit: a digit
+// whose wait runs out stops waiting, and the block then counts that digit's keys in all
+// earlier tiles itself from the pass's input (which the previous launch wrote completely),
+// so the result stays exact; the kernel records kErrSortSpin in the error word to say that
+// a wait ran out.
 #include "internal.cuh"
 
 namespace apo2
@@ -25,7 +29,7 @@ namespace apo2
     constexpr uint32_t kFlagAggregate = 1u << 30;
     constexpr uint32_t kFlagPrefix    = 2u << 30;
     constexpr uint32_t kValueMask     = ( 1u << 30 ) - 1;
-    constexpr uint32_t kSpinLimit     = 1u << 22;
+    constexpr uint32_t kSpinLimit     = 1u << 22; // default polls per look-back wait
 
     static inline size_t align256( size_t b ) { return ( b + 255 ) & ~size_t( 255 ); }
 
@@ -109,6 +113,7 @@ namespace apo2
         uint32_t global_base[ kRadix ];               // global position of the tile's first key per digit
         uint32_t scan_tmp[ kSortWarps ];
         uint32_t tile;
+        uint32_t gave_up; // some digit's look-back wait ran out
     };
 
     __global__ void __launch_bounds__( kSortThreads ) k_onesweep( const uint64_t * __restrict__ keys_in,
@@ -117,14 +122,17 @@ namespace apo2
                                                                   uint32_t * __restrict__ values_out, uint32_t n,
                                                                   uint32_t shift, const uint32_t * __restrict__ digit_offsets,
                                                                   uint32_t * lookback, uint32_t * tile_counter,
-                                                                  uint32_t * error )
+                                                                  uint32_t * error, uint32_t spin_limit )
     {
         extern __shared__ __align__( 16 ) unsigned char smem_raw[];
         OnesweepShared & sh   = *reinterpret_cast<OnesweepShared *>( smem_raw );
         const uint32_t   lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
         if ( threadIdx.x == 0 )
-            sh.tile = atomicAdd( tile_counter, 1u );
+        {
+            sh.tile    = atomicAdd( tile_counter, 1u );
+            sh.gave_up = 0;
+        }
         for ( uint32_t d = threadIdx.x; d < kSortWarps * kRadix; d += kSortThreads )
             ( &sh.warp_counts[ 0 ][ 0 ] )[ d ] = 0;
         __syncthreads();
@@ -185,6 +193,7 @@ namespace apo2
                 atomicExch( slot, kFlagAggregate | count );
 
             uint32_t exclusive = 0;
+            bool     waited_out = false;
             if ( tile > 0 )
             {
                 int32_t  p      = int32_t( tile ) - 1;
@@ -194,9 +203,9 @@ namespace apo2
                     const uint32_t word = __ldcv( lookback + size_t( p ) * kRadix + d );
                     if ( ( word & ~kValueMask ) == 0 )
                     {
-                        if ( ++spins > kSpinLimit )
+                        if ( ++spins > spin_limit )
                         {
-                            atomicOr( error, uint32_t( kErrSortSpin ) );
+                            waited_out = true;
                             break;
                         }
                         __nanosleep( 32 );
@@ -207,7 +216,30 @@ namespace apo2
                         break;
                     p--;
                 }
-                atomicExch( slot, kFlagPrefix | ( ( exclusive + count ) & kValueMask ) );
+                if ( waited_out )
+                    sh.gave_up = 1; // this digit's prefix is counted below, then published
+                else
+                    atomicExch( slot, kFlagPrefix | ( ( exclusive + count ) & kValueMask ) );
+            }
+            __syncthreads();
+            if ( sh.gave_up )
+            {
+                // Exact fallback: count the digits of every key in tiles [0, tile) from the
+                // pass's input. tile_prefix serves as the counter array until the scan below.
+                sh.tile_prefix[ d ] = 0;
+                __syncthreads();
+                const uint32_t end = min( n, tile * kTile );
+                for ( uint32_t i = threadIdx.x; i < end; i += kSortThreads )
+                    atomicAdd( &sh.tile_prefix[ uint32_t( ( keys_in[ i ] >> shift ) & ( kRadix - 1 ) ) ], 1u );
+                __syncthreads();
+                if ( waited_out )
+                {
+                    exclusive = sh.tile_prefix[ d ];
+                    atomicExch( slot, kFlagPrefix | ( ( exclusive + count ) & kValueMask ) );
+                }
+                if ( threadIdx.x == 0 )
+                    atomicOr( error, uint32_t( kErrSortSpin ) );
+                __syncthreads();
             }
             sh.global_base[ d ] = digit_offsets[ d ] + exclusive;
 
@@ -257,16 +289,17 @@ namespace apo2
         }
     }
 
-    void radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t n, SortScratch & s, cudaStream_t stream )
+    void radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t n, SortScratch & s, cudaStream_t stream,
+                           uint32_t spin_limit )
     {
         if ( n < 2 )
             return;
-        static bool configured = false;
-        if ( !configured )
-        {
+        // the tile's shared memory is above the 48 KB default: the attribute is set once per
+        // device, on the device current when the sort is launched
+        static PerDeviceOnce configured;
+        configured.run( [] {
             cudaFuncSetAttribute( k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, int( sizeof( OnesweepShared ) ) );
-            configured = true;
-        }
+        } );
         const uint32_t tiles = tiles_for( n );
         cudaMemsetAsync( s.histograms, 0, sizeof( uint32_t ) * kPasses * kRadix, stream );
         cudaMemsetAsync( s.tile_counter, 0, sizeof( uint32_t ) * kPasses, stream );
@@ -282,7 +315,8 @@ namespace apo2
         {
             cudaMemsetAsync( s.lookback, 0, sizeof( uint32_t ) * size_t( tiles ) * kRadix, stream );
             APO2_LAUNCH( "k_onesweep", stream, k_onesweep<<<tiles, kSortThreads, sizeof( OnesweepShared ), stream>>>(
-                kin, vin, kout, vout, n, p * kRadixBits, s.histograms + p * kRadix, s.lookback, s.tile_counter + p, s.error ) );
+                kin, vin, kout, vout, n, p * kRadixBits, s.histograms + p * kRadix, s.lookback, s.tile_counter + p, s.error,
+                spin_limit ? spin_limit : kSpinLimit ) );
             std::swap( kin, kout );
             std::swap( vin, vout );
         }

@@ -83,7 +83,11 @@ typedef struct apo2_options
                                       diagram's, and the shards' outputs in shard order are the whole
                                       diagram's output, in order */
     uint32_t shard_count;
-    uint32_t reserved[ 6 ];
+    uint32_t wait_limit;           /* polls per look-back wait of the LBVH's radix sort before the tile
+                                      counts its digits itself (exact either way; 0 = 2^22). Tests set
+                                      it small to exercise that path; apo2_stats.error_flags bit 32
+                                      reports that a wait ran out */
+    uint32_t reserved[ 5 ];
 } apo2_options;
 
 #define APO2_NO_KNN_STEPS 0xffffffffu
@@ -95,8 +99,9 @@ typedef struct apo2_stats
     uint32_t buried;               /* cells of sites inside another site */
     uint32_t certified_after_knn;  /* cells certified by the kNN security radius */
     uint32_t validation_rounds;    /* vertex+edge validation rounds that had work */
-    uint32_t error_flags;          /* capacity flags (1 vertex, 2 edge, 4 new edge, 8 bisector, 16 stack,
-                                      32 sort look-back, 64 walk or restart bound) */
+    uint32_t error_flags;          /* capacity flags (1 vertex, 2 edge, 4 new edge, 8 bisector, 16 stack),
+                                      32 a sort look-back wait ran out (recounted: the order is exact),
+                                      64 a walk or restart loop reached its bound */
     uint32_t kernel_launches;      /* kernels launched by the last build (+ extraction) */
     uint64_t vertex_records;       /* sum of per-cell vertex counts */
     uint64_t edge_records;         /* sum of per-cell edge counts */
@@ -112,6 +117,8 @@ typedef struct apo2_stats
     double   ms_bisector_validation;
     double   ms_output;
     uint64_t device_bytes;         /* device memory held by the handle */
+    uint32_t uncertified;          /* cells still in validation after the last round (APO2_ERR_ITER_LIMIT) */
+    uint32_t reserved32;
 } apo2_stats;
 
 /* Library version string. */
@@ -132,7 +139,11 @@ apo2_status apo2_set_sites( apo2_handle * h, const void * sites, apo2_dtype dtyp
                             void * stream );
 
 /* Builds the diagram on `stream` (a cudaStream_t; 0 = default). Asynchronous with respect to
- * the host unless `synchronize` is non-zero, in which case the error flags are checked.
+ * the host unless `synchronize` is non-zero, in which case the build's status is returned:
+ * APO2_ERR_CAPACITY when a per-cell store overflowed, APO2_ERR_ITER_LIMIT when cells were still
+ * uncertified after max_iterations validation rounds (or a bounded walk stopped early). The
+ * diagram is complete in both cases, as the reference leaves it (the reference prints or ignores
+ * these conditions); apo2_get_stats gives the flags and the uncertified count.
  * Replaces: AlgorithmGPU<K>::build() (apo/include/apo/gpu/algorithm.inl:1410-1594). */
 apo2_status apo2_build( apo2_handle * h, void * stream, int synchronize );
 
@@ -184,6 +195,21 @@ apo2_status apo2_topology_json( apo2_handle * h, char * json, uint64_t capacity,
  * search walks the handle's BVH instead of all sites. */
 apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint32_t * ids, uint64_t count, uint32_t arity,
                           apo2_location location, uint8_t * flags, uint64_t * bad );
+
+/* Error of output vertices against an FP64 oracle, per result: each vertex (x, y, z, w) with its
+ * four original site ids is refined by Newton steps on |p - c_a| - r_a - w = 0 (a = the four
+ * sites) in IEEE double precision, and its error is max over x, y, z, w of
+ * |given - refined| / max(1, |refined|). The reference computes vertices in double precision but
+ * with a single-precision square root inside every length (gpu/math.cuh:307-309); the required
+ * bound for every result is 1e-5. positions/ids: double[4*count] / uint32[4*count] on the host
+ * or the device, or both NULL for the handle's last extracted vertices (count is then taken
+ * from it). errors (optional, host float[count]) receives each vertex's error; *max_error the
+ * largest; *above (optional) how many exceed `threshold`; *singular (optional) how many
+ * vertices have a singular system (their error is reported as 0). No counterpart in the
+ * reference, whose precision harness (app/precision/precision.cpp) checks emptiness only. */
+apo2_status apo2_vertex_error( apo2_handle * h, const double * positions, const uint32_t * ids, uint64_t count,
+                               apo2_location location, double threshold, float * errors, double * max_error,
+                               uint64_t * above, uint64_t * singular );
 
 /* Labels of the kNN cell construction, as the reference's measurement harness records them
  * (app/benchmarks/benchmark_contributing_nearest.cu:10-129): `steps` kNN steps of the handle's K
@@ -271,7 +297,10 @@ apo2_status apo2_lbvh_build( const float * sites_xyzr, uint32_t n, const float s
                              void * scratch, void * stream );
 
 /* Stable radix sort of (u64 key, u32 value) pairs by key on the device (the LBVH's sort):
- * keys/values are sorted in place; `scratch` must hold apo2_radix_sort_scratch_bytes(n). */
+ * keys/values are sorted in place; `scratch` must hold apo2_radix_sort_scratch_bytes(n). Its
+ * first 4 bytes receive the sort's status word on the stream: 0, or 32 when a look-back wait
+ * ran out and the tile counted its digits itself (the order is exact either way). The same
+ * holds for apo2_lbvh_build's scratch. */
 uint64_t    apo2_radix_sort_scratch_bytes( uint32_t n );
 apo2_status apo2_radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t n, void * scratch, void * stream );
 

@@ -13,7 +13,7 @@ Cases may set the AlgorithmGPU<K> template argument and the knnValidationStep co
 argument (default 16 and 1); the driver gets them as --k / --knn-steps.
 
 Usage:
-    python tests/golden/make_golden.py inputs <dir>   writes <case>.f32 and <case>.args per case
+    python tests/golden/make_golden.py inputs <dir> [case ...]   writes <case>.f32 and <case>.args
     bash tests/golden/dump_reference.sh <dir> <dump_root>   (on a GPU: runs the reference driver)
     python tests/golden/make_golden.py <dump_root>    (dump_root/<case>/*.u32 ...) -> fixtures
 """
@@ -53,6 +53,13 @@ CASES = {
     "uni100k": ("uniform_cloud(100000, 215.44, 1.5, 0.5)", False),
     "logn50k": ("lognormal_cloud(50000, 400.0 * (0.01 ** (1 / 3)), seed=9)", False),
     "protein100k": ("protein_chains(200, 500, 0.01, seed=1)", False),
+    # full-size pins: the bench's 1M protein-like packing (config 1), the near-degenerate
+    # lattices at 50^3 (config 2 A/B at the largest size the reference finishes in minutes)
+    # and a 500,000-site log-normal cloud at the density of the 5M evaluation cloud (config 3)
+    "protein1m": ("protein_chains(2000, 500, 0.01, seed=1)", False),
+    "latticeA50": ("lattice(50, 'A', seed=6)", False),
+    "latticeB50": ("lattice(50, 'B', seed=7)", False),
+    "logn500k": ("lognormal_cloud(500000, 400.0 * (0.1 ** (1 / 3)), seed=11)", False),
 }
 
 
@@ -92,9 +99,9 @@ def digest(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def write_inputs(out: str) -> None:
+def write_inputs(out: str, cases: list[str] | None = None) -> None:
     os.makedirs(out, exist_ok=True)
-    for case in CASES:
+    for case in cases or list(CASES):
         sites_for(case).astype(np.float32).tofile(os.path.join(out, case + ".f32"))
         k, steps = case_params(case)
         with open(os.path.join(out, case + ".args"), "w") as f:
@@ -133,6 +140,6 @@ def main(root: str) -> None:
 
 if __name__ == "__main__":
     if sys.argv[1] == "inputs":
-        write_inputs(sys.argv[2])
+        write_inputs(sys.argv[2], sys.argv[3:] or None)
     else:
         main(sys.argv[1])

@@ -85,8 +85,9 @@ def _struct_layout_program() -> str:
 int main(void) {
     printf("apo2_options %zu\n", sizeof(apo2_options));
     printf("apo2_stats %zu\n", sizeof(apo2_stats));
-    F(apo2_options, k) F(apo2_options, edge_search) F(apo2_options, reserved)
+    F(apo2_options, k) F(apo2_options, edge_search) F(apo2_options, wait_limit) F(apo2_options, reserved)
     F(apo2_stats, vertex_records) F(apo2_stats, ms_bounds) F(apo2_stats, ms_output) F(apo2_stats, device_bytes)
+    F(apo2_stats, uncertified)
     return 0;
 }
 """

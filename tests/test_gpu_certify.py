@@ -68,3 +68,40 @@ def test_certificate_flags_a_displaced_vertex():
     assert bad == moved.size
     assert np.array_equal(brute_force_bad(sites, pos, ids, 4), flags.astype(bool))
     algo.close()
+
+
+def _newton_refine(sites, pos, ids):
+    """numpy restatement of the vertex-error oracle: Newton steps on |p - c_a| - r_a - w = 0."""
+    x = pos.astype(np.float64).copy()
+    s = sites.astype(np.float64)[ids.astype(np.int64)]  # (Q, 4 sites, 4)
+    for _ in range(4):
+        d = x[:, None, :3] - s[:, :, :3]
+        dist = np.sqrt((d * d).sum(axis=2))
+        jac = np.concatenate([d / dist[:, :, None], -np.ones(dist.shape + (1,))], axis=2)
+        f = dist - s[:, :, 3] - x[:, 3:4]
+        x = x - np.linalg.solve(jac, f[:, :, None])[:, :, 0]
+    return x
+
+
+def test_vertex_error_against_fp64_refinement():
+    """Per-result error of the output vertices (bound 1e-5 relative) against a numpy restatement
+    of the refinement; a vertex moved by 1e-3 shows an error of that size."""
+    import apo_b200
+    sites = H.sites_for("uni2k")
+    algo = apo_b200.AlgorithmGPU(sites)
+    algo.build()
+    v = algo.toHost()
+    pos = v.vertices.reshape(-1, 4)
+    ids = v.verticesId.reshape(-1, 4)
+    mx, above, singular, errs = algo.vertex_error()
+    assert singular == 0
+    assert mx <= 1e-5 and above == 0, mx
+    ref = _newton_refine(sites, pos, ids)
+    ref_err = np.max(np.abs(pos - ref) / np.maximum(1.0, np.abs(ref)), axis=1)
+    assert np.allclose(errs, ref_err, rtol=1e-3, atol=1e-12)
+    moved = pos.copy()
+    moved[7, 0] += 1e-3 * max(1.0, abs(moved[7, 0]))
+    mx2, above2, _, errs2 = algo.vertex_error(moved, ids)
+    assert above2 == 1 and np.argmax(errs2) == 7
+    assert 0.5e-3 < mx2 < 2e-3
+    algo.close()
