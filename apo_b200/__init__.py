@@ -59,7 +59,8 @@ class Stats(ctypes.Structure):
                 ("ms_knn", ctypes.c_double), ("ms_cells", ctypes.c_double), ("ms_vertex_validation", ctypes.c_double),
                 ("ms_edge_validation", ctypes.c_double), ("ms_bisector_validation", ctypes.c_double),
                 ("ms_output", ctypes.c_double), ("device_bytes", ctypes.c_uint64), ("uncertified", ctypes.c_uint32),
-                ("reserved32", ctypes.c_uint32)]
+                ("reserved32", ctypes.c_uint32), ("knn_insertions", ctypes.c_uint64), ("proposal_cells", ctypes.c_uint64),
+                ("proposal_fallbacks", ctypes.c_uint64), ("proposal_skipped", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("reserved")}
@@ -95,10 +96,16 @@ SIGNATURES = {
     "apo2_radix_sort_pairs": (_I, [_P, _P, _U32, _P, _P]),
     "apo2_radix_sort_pairs_static": (_I, [_P, _P, _U32, _P]),
     "apo2_generate_chains": (_I, [_U32, _U32, ctypes.c_double, _U64, _P]),
+    "apo2_fma_peak": (_I, [_P, _P]),
     "apo2_topology_json": (_I, [_P, _P, _U64, _P]),
     "apo2_certify": (_I, [_P, _P, _P, _U64, _U32, _I, _P, _P]),
     "apo2_contribution_profile": (_I, [_P, _U32, _P, _P]),
     "apo2_vertex_error": (_I, [_P, _P, _P, _U64, _I, ctypes.c_double, _P, _P, _P, _P]),
+    "apo2_proposal_features": (_I, [_P, _P]),
+    "apo2_proposal_predict": (_I, [_P, _P, _U64, _P]),
+    "apo2_proposal_gradients": (_I, [_P, _P, _P, _P, _U32, _P, _P]),
+    "apo2_proposal_train": (_I, [_P, _P, _U64, _U32, _U32, ctypes.c_float, _U64, _P, _P, _P]),
+    "apo2_set_proposal": (_I, [_P, _P]),
     "apo2_batch_create": (_I, [_U32, _U32, _P, _P]),
     "apo2_batch_build": (_I, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "apo2_batch_destroy": (_I, [_P]),
@@ -436,6 +443,13 @@ def computeApolloniusDiagram(sites) -> VertexDiagram:
         lib.apo2_free(pos)
         lib.apo2_free(ids)
     return VertexDiagram(vertices=p, verticesId=i)
+
+
+def fma_peak() -> tuple[float, float]:
+    """Measured FP64 and FP32 FMA-pipe peaks of the current device, TFLOP/s."""
+    f64, f32 = ctypes.c_double(), ctypes.c_double()
+    _check(load_library().apo2_fma_peak(ctypes.byref(f64), ctypes.byref(f32)))
+    return f64.value, f32.value
 
 
 def getDirections(count: int = 64) -> np.ndarray:

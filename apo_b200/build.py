@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libapo2.so")
-SOURCES = ["sort.cu", "lbvh.cu", "cells.cu", "speculate.cu", "certify.cu", "cavity.cu", "api.cu", "sort_static.cu", "generators.cpp"]
+SOURCES = ["sort.cu", "lbvh.cu", "cells.cu", "speculate.cu", "certify.cu", "cavity.cu", "api.cu", "sort_static.cu", "calibrate.cu", "proposal.cu", "generators.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--use_fast_math", "-Xcompiler", "-fPIC,-O2",
          "-I", os.path.join(ROOT, "include")]

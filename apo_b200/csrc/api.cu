@@ -103,6 +103,9 @@ struct apo2_handle
     uint64_t extract_epoch = 0;
     uint64_t ratio_epoch   = ~0ull;
 
+    // learned k-proposal: the network on the device and the proposed rank of every site
+    void * proposal_alloc = nullptr;
+
     cudaEvent_t events[ kStages + 1 ] = {};
     bool        timing                = false;
     apo2_stats  stats {};
@@ -215,6 +218,7 @@ namespace
         h->records.clear();
         record( h, 0, s );
         cudaMemsetAsync( h->error, 0, sizeof( uint32_t ), s );
+        cudaMemsetAsync( h->cells.counters, 0, sizeof( unsigned long long ) * kCounters, s );
         launch_bounds( h->input, h->input_f64, n, h->input_d4, h->partials, h->partial_count, h->bounds_counter, h->scene,
                        h->tree.sites + n, s );
         record( h, 1, s );
@@ -394,6 +398,7 @@ namespace
         total += align256( 4 * size_t( n ) ) * 2 + align256( 4 * scanWords * 2 ) + align256( 16 );
         total += align256( spec_bytes( n ) );
         total += align256( walk_scratch_bytes() ) + align256( 4 );
+        total += align256( sizeof( unsigned long long ) * kCounters );
         return total;
     }
 
@@ -455,6 +460,8 @@ namespace
         spec_carve( h->spec, a.take<char>( spec_bytes( n ) ), n );
         c.walk_scratch    = a.take<uint32_t>( walk_scratch_bytes() / sizeof( uint32_t ) );
         c.work_counter    = a.take<uint32_t>( 1 );
+        c.counters        = a.take<unsigned long long>( kCounters );
+        c.codes           = t.codes;
         sort_scratch_carve( h->sort, sortBase, n, h->error );
         return a.used <= a.size;
     }
@@ -1267,6 +1274,12 @@ apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
         s.validation_rounds += counts[ r ] != 0;
     s.error_flags     = err;
     s.uncertified     = h->options.stop_after == 0 ? counts[ h->options.max_iterations ] : 0;
+    unsigned long long cnt[ kCounters ] = {};
+    cudaMemcpy( cnt, h->cells.counters, sizeof( cnt ), cudaMemcpyDeviceToHost );
+    s.knn_insertions     = cnt[ kCountInsertions ];
+    s.proposal_cells     = cnt[ kCountChecked ];
+    s.proposal_fallbacks = cnt[ kCountFallbacks ];
+    s.proposal_skipped   = cnt[ kCountSkipped ];
     s.kernel_launches = h->launches;
     if ( h->timing )
     {
@@ -1323,6 +1336,58 @@ apo2_status apo2_kernel_profile( apo2_handle * h, char * json, uint64_t capacity
     return APO2_OK;
 }
 
+apo2_status apo2_set_proposal( apo2_handle * h, const apo2_proposal * model )
+{
+    if ( !h || ( model && ( model->struct_size != sizeof( apo2_proposal ) || model->version != 1 ) ) )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_set_proposal" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    APO2_CUDA( cudaDeviceSynchronize(), "set proposal" ); // no build may still read the old model
+    if ( !model )
+    {
+        h->cells.proposal   = nullptr;
+        h->cells.proposed_k = nullptr;
+        return APO2_OK;
+    }
+    if ( !h->proposal_alloc )
+        APO2_CUDA( cudaMalloc( &h->proposal_alloc, align256( sizeof( ProposalNet ) ) + align256( h->n ) ), "proposal allocation" );
+    char * p = static_cast<char *>( h->proposal_alloc );
+    APO2_CUDA( cudaMemcpy( p, reinterpret_cast<const char *>( model ) + 2 * sizeof( uint32_t ), sizeof( ProposalNet ),
+                           cudaMemcpyHostToDevice ),
+               "proposal upload" );
+    h->cells.proposal   = reinterpret_cast<const ProposalNet *>( p );
+    h->cells.proposed_k = reinterpret_cast<uint8_t *>( p + align256( sizeof( ProposalNet ) ) );
+    return APO2_OK;
+}
+
+apo2_status apo2_proposal_features( apo2_handle * h, float * features )
+{
+    if ( !h || !features )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_proposal_features" );
+    if ( !h->built )
+        return fail( APO2_ERR_NOT_BUILT, "no build yet" );
+    if ( h->options.knn_steps != 1 )
+        return fail( APO2_ERR_INVALID_ARG, "features need the first kNN step's lists (knn_steps = 1)" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    float * d = nullptr;
+    APO2_CUDA( cudaMalloc( &d, sizeof( float ) * kPIn * size_t( h->n ) ), "features allocation" );
+    FeatureInputs in;
+    in.sites_f = h->cells.sites_f;
+    in.codes   = h->cells.codes;
+    in.scene   = h->scene;
+    in.n       = h->n;
+    {
+        ObserveScope observe( h );
+        launch_features( in, h->cells.knn, h->cells.k, d, 0 );
+    }
+    cudaError_t e = cudaGetLastError();
+    if ( e == cudaSuccess )
+        e = cudaMemcpy( features, d, sizeof( float ) * kPIn * size_t( h->n ), cudaMemcpyDeviceToHost );
+    cudaFree( d );
+    if ( e != cudaSuccess )
+        return cuda_fail( e, "features" );
+    return APO2_OK;
+}
+
 apo2_status apo2_destroy( apo2_handle * h )
 {
     if ( !h )
@@ -1333,6 +1398,8 @@ apo2_status apo2_destroy( apo2_handle * h )
         cudaFree( h->out_alloc );
     if ( h->cavity_alloc )
         cudaFree( h->cavity_alloc );
+    if ( h->proposal_alloc )
+        cudaFree( h->proposal_alloc );
     if ( h->arena.base )
         cudaFree( h->arena.base );
     if ( h->timing )

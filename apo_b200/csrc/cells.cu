@@ -681,11 +681,24 @@ namespace apo2
     // kNN step `step` (algorithm.inl:32-99): step 0 takes the k nearest sites and flags buried
     // sites; a later step takes the next k, beyond the last neighbour of the previous step, or
     // none once the previous list ran short.
+    // Propose: the learned form's first step, which also runs the k-proposal network (a separate
+    // instantiation, so that the plain search keeps its small register footprint).
+    template<bool Propose>
     __global__ void __launch_bounds__( kKnnBlock ) k_knn( CellContext c, uint32_t step )
     {
-        __shared__ uint32_t s_keys[ kMaxK * kKnnBlock ];
-        __shared__ float    s_dist[ kMaxK * kKnnBlock ];
-        const uint32_t      id = blockIdx.x * blockDim.x + threadIdx.x;
+        __shared__ uint32_t    s_keys[ kMaxK * kKnnBlock ];
+        __shared__ float       s_dist[ kMaxK * kKnnBlock ];
+        extern __shared__ __align__( 16 ) unsigned char s_dyn[]; // the network (Propose only)
+        ProposalNet *          s_net   = reinterpret_cast<ProposalNet *>( s_dyn );
+        constexpr bool         propose = Propose;
+        if ( propose )
+        {
+            // the network, staged once per block (broadcast reads during inference)
+            for ( uint32_t t = threadIdx.x; t < sizeof( ProposalNet ) / 4; t += blockDim.x )
+                reinterpret_cast<uint32_t *>( s_net )[ t ] = reinterpret_cast<const uint32_t *>( c.proposal )[ t ];
+            __syncthreads();
+        }
+        const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
         if ( id >= c.n )
             return;
         const uint32_t k      = c.k;
@@ -794,6 +807,18 @@ namespace apo2
             atomicOr( c.error, err );
         if ( step != 0 )
             return;
+        if ( propose )
+        {
+            // fused inference of the k-proposal on the sorted list
+            FeatureInputs in;
+            in.sites_f = c.sites_f;
+            in.codes   = c.codes;
+            in.scene   = c.scene;
+            in.n       = n;
+            float f[ kPIn ];
+            proposal_features( in, id, keys, stride, k, f );
+            c.proposed_k[ id ] = uint8_t( proposal_rank( s_net[ 0 ], proposal_predict( s_net[ 0 ], f ), k ) );
+        }
 
         // buried site: inside its nearest neighbour (algorithm.inl:85-98); `si` is the float copy
         const uint32_t nearest = keys[ 0 ];
@@ -846,6 +871,12 @@ namespace apo2
         const uint32_t nwarp = gridDim.x * ( kCellBlock / 32 );
         WarpCell       w     = carve( smem, warp, 0 );
         uint32_t       err   = 0;
+        // per-warp counters (lane 0 counts), added to the build's counters at the end
+        __shared__ uint32_t s_counts[ kCellBlock / 32 ][ kCounters ];
+        uint32_t *          counts = s_counts[ warp ];
+        if ( lane_id() < kCounters )
+            counts[ lane_id() ] = 0;
+        __syncwarp();
         // cells are taken one at a time from a shared counter (uneven cells, see bisector pass)
         ( void ) gwarp;
         ( void ) nwarp;
@@ -884,22 +915,47 @@ namespace apo2
                 __syncwarp();
                 continue;
             }
-            double known = -DBL_MAX;
+            // learned form: the certificate is first checked at the proposed rank; a cell that
+            // passes there stops inserting (its later neighbours cannot change a certified cell)
+            // but its known radius still covers its whole list, as the plain form's does
+            const uint32_t check_at = ( c.proposed_k && mode == kCellsFirst ) ? c.proposed_k[ i ] : c.k;
+            double         known    = -DBL_MAX;
+            bool           done     = false;
             for ( uint32_t q = 0; q < c.k; q++ )
             {
+                if ( q == check_at )
+                {
+                    const double radius = cell_radius( c, w, si );
+                    done                = gt_eps( known, 2.0 * radius );
+                    if ( lane_id() == 0 )
+                        counts[ kCountChecked ]++;
+                    if ( !done && lane_id() == 0 )
+                        counts[ kCountFallbacks ]++;
+                }
                 const uint32_t j = c.knn[ size_t( i ) * c.k + q ];
                 if ( j == kNone )
                     break;
                 if ( c.status[ j ] == kBuried )
                     continue;
                 const double4 sj = c.sites[ j ];
-                update_cell( c, w, i, si, j, sj, err );
+                if ( done )
+                {
+                    if ( lane_id() == 0 )
+                        counts[ kCountSkipped ]++;
+                }
+                else
+                {
+                    update_cell( c, w, i, si, j, sj, err );
+                    if ( lane_id() == 0 )
+                        counts[ kCountInsertions ]++;
+                }
                 known = fmax( known, sphere_distance( si, sj ) );
             }
-            const double radius = cell_radius( c, w, si );
+            if ( !done )
+                done = gt_eps( known, 2.0 * cell_radius( c, w, si ) );
             if ( lane_id() == 0 )
             {
-                if ( gt_eps( known, 2.0 * radius ) )
+                if ( done )
                     c.status[ i ] = kFullyValidated;
                 c.known_radii[ i ] = float( known );
             }
@@ -907,6 +963,11 @@ namespace apo2
             __syncwarp();
         }
         report( c, err );
+        __syncwarp();
+        if ( c.counters && lane_id() == 0 )
+            for ( uint32_t t = 0; t < kCounters; t++ )
+                if ( counts[ t ] )
+                    atomicAdd( c.counters + t, static_cast<unsigned long long>( counts[ t ] ) );
     }
 
     // Per-neighbour labels of the kNN cell construction (the reference's measurement harness
@@ -2242,7 +2303,11 @@ namespace apo2
 
     void launch_knn( const CellContext & c, uint32_t step, cudaStream_t s )
     {
-        APO2_LAUNCH( "k_knn", s, k_knn<<<( c.n + kKnnBlock - 1 ) / kKnnBlock, kKnnBlock, 0, s>>>( c, step ) );
+        const uint32_t blocks = ( c.n + kKnnBlock - 1 ) / kKnnBlock;
+        if ( c.proposal && step == 0 )
+            APO2_LAUNCH( "k_knn_propose", s, k_knn<true><<<blocks, kKnnBlock, sizeof( ProposalNet ), s>>>( c, step ) );
+        else
+            APO2_LAUNCH( "k_knn", s, k_knn<false><<<blocks, kKnnBlock, 0, s>>>( c, step ) );
     }
 
     void launch_cells( const CellContext & c, uint32_t mode, cudaStream_t s )

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "internal.cuh"
+#include "proposal.cuh"
 
 namespace apo2
 {
@@ -42,7 +43,15 @@ namespace apo2
         const Scene *    scene       = nullptr; // bounds and radius range of the sites
         uint32_t *       walk_scratch = nullptr; // kWalkScratchWords per warp of the exact edge pass
         uint32_t *       work_counter = nullptr; // next cell of the dynamically scheduled passes
+        // learned k-proposal (null: the plain form): the network, the Morton codes its features
+        // read, and the proposed rank of every site (written by the first kNN step)
+        const ProposalNet * proposal   = nullptr;
+        const uint64_t *    codes      = nullptr;
+        uint8_t *           proposed_k = nullptr;
+        // build counters: kNN insertions, cells checked at a proposed rank, fallbacks, skipped neighbours
+        unsigned long long * counters = nullptr;
     };
+    constexpr uint32_t kCountInsertions = 0, kCountChecked = 1, kCountFallbacks = 2, kCountSkipped = 3, kCounters = 4;
 
     // Row of cell i in the per-cell stores (vertices, edges), which hold only the cells
     // [lo, hi) a handle builds: a shard of the diagram needs stores for its own cells alone.

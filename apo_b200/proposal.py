@@ -1,0 +1,194 @@
+"""Learned k-proposal of the kNN cell construction: model type, training data and training.
+
+The network (16 -> 64 -> 64 -> 1, ReLU, bf16 weights, fp32 accumulation) predicts log2 of the
+kNN rank at which a site's cell passes the security-radius certificate. Everything that runs on
+the GPU -- the feature extraction, the inference fused into the kNN kernel, the training
+forward / backward / Adam kernels -- is in the CUDA library (apo_b200/csrc/proposal.cu, the C
+ABI in include/apo2.h); this module prepares data and drives the calls.
+
+Labels are the reference's own measurement (app/benchmarks/benchmark_contributing_nearest.cu:
+10-129, restated as apo2_contribution_profile): the rank at which the certificate first held
+during the plain construction. A cell that does not certify within the list gets the label
+log2(K) + 1 (its proposal is then the whole list, which is the plain form).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import AlgorithmGPU, _check, load_library
+
+INPUTS, HIDDEN = 16, 64
+PARAMS = HIDDEN * INPUTS + HIDDEN + HIDDEN * HIDDEN + HIDDEN + HIDDEN + 1  # 5,313
+DEFAULT_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "proposal_k16.npz")
+
+
+class Proposal(ctypes.Structure):
+    """apo2_proposal (include/apo2.h)."""
+    _fields_ = [("struct_size", ctypes.c_uint32), ("version", ctypes.c_uint32),
+                ("mean", ctypes.c_float * INPUTS), ("inv_scale", ctypes.c_float * INPUTS),
+                ("margin", ctypes.c_float), ("b3", ctypes.c_float),
+                ("b1", ctypes.c_float * HIDDEN), ("b2", ctypes.c_float * HIDDEN),
+                ("w1", ctypes.c_uint16 * (HIDDEN * INPUTS)), ("w2", ctypes.c_uint16 * (HIDDEN * HIDDEN)),
+                ("w3", ctypes.c_uint16 * HIDDEN)]
+
+
+def _sig():
+    return load_library()
+
+
+class Model:
+    """A trained (or initial) network: the fp32 parameter vector and the bf16 model the GPU reads."""
+
+    def __init__(self, master: np.ndarray, mean: np.ndarray, inv_scale: np.ndarray, margin: float = 0.0):
+        self.master = np.ascontiguousarray(master, dtype=np.float32)
+        assert self.master.size == PARAMS
+        self.mean = np.ascontiguousarray(mean, dtype=np.float32)
+        self.inv_scale = np.ascontiguousarray(inv_scale, dtype=np.float32)
+        self.margin = float(margin)
+
+    @staticmethod
+    def initial(features: np.ndarray, seed: int = 0) -> "Model":
+        """He-initialised weights, zero biases, inputs standardised on `features`."""
+        rng = np.random.default_rng(seed)
+        mean = features.mean(axis=0)
+        std = features.std(axis=0)
+        inv = 1.0 / np.where(std > 1e-6, std, 1.0)
+        w1 = rng.normal(0, np.sqrt(2.0 / INPUTS), (HIDDEN, INPUTS))
+        w2 = rng.normal(0, np.sqrt(2.0 / HIDDEN), (HIDDEN, HIDDEN))
+        w3 = rng.normal(0, np.sqrt(1.0 / HIDDEN), HIDDEN)
+        master = np.concatenate([w1.ravel(), np.zeros(HIDDEN), w2.ravel(), np.zeros(HIDDEN), w3, [0.0]])
+        return Model(master, mean, inv)
+
+    def struct(self) -> Proposal:
+        """The apo2_proposal of this model (bf16 weights rounded to nearest even from the master)."""
+        from_master = _bf16_bits(self.master)
+        p = Proposal()
+        p.struct_size = ctypes.sizeof(Proposal)
+        p.version = 1
+        p.mean[:] = self.mean.tolist()
+        p.inv_scale[:] = self.inv_scale.tolist()
+        p.margin = self.margin
+        o = 0
+        w1 = from_master[o:o + HIDDEN * INPUTS]; o += HIDDEN * INPUTS
+        b1 = self.master[o:o + HIDDEN]; o += HIDDEN
+        w2 = from_master[o:o + HIDDEN * HIDDEN]; o += HIDDEN * HIDDEN
+        b2 = self.master[o:o + HIDDEN]; o += HIDDEN
+        w3 = from_master[o:o + HIDDEN]; o += HIDDEN
+        p.w1[:] = w1.tolist()
+        p.b1[:] = b1.tolist()
+        p.w2[:] = w2.tolist()
+        p.b2[:] = b2.tolist()
+        p.w3[:] = w3.tolist()
+        p.b3 = float(self.master[o])
+        return p
+
+    def predict(self, features: np.ndarray) -> np.ndarray:
+        """log2-rank predictions of the GPU network (apo2_proposal_predict)."""
+        lib = _sig()
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        out = np.zeros(x.shape[0], dtype=np.float32)
+        p = self.struct()
+        _check(lib.apo2_proposal_predict(ctypes.byref(p), x.ctypes.data, x.shape[0], out.ctypes.data))
+        return out
+
+    def ranks(self, features: np.ndarray, k: int = 16) -> np.ndarray:
+        """Proposed ranks ceil(2^(prediction + margin)) in [1, k], as the kNN kernel computes them."""
+        pred = self.predict(features).astype(np.float32)
+        r = np.ceil(np.exp2(np.minimum(pred + np.float32(self.margin), 30.0)))
+        return np.clip(r, 1, k).astype(np.int64)
+
+    def gradients(self, features: np.ndarray, targets: np.ndarray) -> tuple[float, np.ndarray]:
+        """Loss and gradient of one batch from the GPU training kernels."""
+        lib = _sig()
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        y = np.ascontiguousarray(targets, dtype=np.float32)
+        g = np.zeros(PARAMS, dtype=np.float32)
+        loss = ctypes.c_float()
+        p = self.struct()
+        _check(lib.apo2_proposal_gradients(ctypes.byref(p), self.master.ctypes.data, x.ctypes.data, y.ctypes.data, x.shape[0],
+                                           ctypes.byref(loss), g.ctypes.data))
+        return loss.value, g
+
+    def train(self, features: np.ndarray, targets: np.ndarray, epochs: int = 8, batch: int = 4096, lr: float = 2e-3,
+              seed: int = 1) -> np.ndarray:
+        """Trains in place on the GPU (apo2_proposal_train); returns the per-epoch mean loss."""
+        lib = _sig()
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        y = np.ascontiguousarray(targets, dtype=np.float32)
+        losses = np.zeros(epochs, dtype=np.float32)
+        p = self.struct()
+        master = self.master.copy()
+        _check(lib.apo2_proposal_train(x.ctypes.data, y.ctypes.data, x.shape[0], epochs, batch, lr, seed,
+                                       master.ctypes.data, ctypes.byref(p), losses.ctypes.data))
+        self.master = master
+        return losses
+
+    def save(self, path: str) -> None:
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        np.savez(path, master=self.master, mean=self.mean, inv_scale=self.inv_scale, margin=np.float32(self.margin))
+
+    @staticmethod
+    def load(path: str = DEFAULT_MODEL) -> "Model":
+        with np.load(path) as z:
+            return Model(z["master"], z["mean"], z["inv_scale"], float(z["margin"]))
+
+
+def _bf16_bits(a: np.ndarray) -> np.ndarray:
+    bits = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    return (((bits + 0x7FFF + ((bits >> 16) & 1)) >> 16) & 0xFFFF).astype(np.uint16)
+
+
+def attach(algo: AlgorithmGPU, model: Model | None) -> None:
+    """Uses `model` for the next builds of `algo` (None: the plain form)."""
+    lib = _sig()
+    if model is None:
+        _check(lib.apo2_set_proposal(algo.handle, None))
+        return
+    p = model.struct()
+    _check(lib.apo2_set_proposal(algo.handle, ctypes.byref(p)))
+
+
+def features(algo: AlgorithmGPU) -> np.ndarray:
+    """(n, 16) float32 features of a built single-step handle, sorted order."""
+    lib = _sig()
+    out = np.zeros((algo.n, INPUTS), dtype=np.float32)
+    _check(lib.apo2_proposal_features(algo.handle, out.ctypes.data))
+    return out
+
+
+def labels(certified_k: np.ndarray, k: int = 16) -> np.ndarray:
+    """log2 of the certified rank (1..k), log2(k) + 1 for cells that did not certify."""
+    ck = np.asarray(certified_k)
+    return np.where(ck > 0, np.log2(np.maximum(ck, 1)), np.log2(k) + 1.0).astype(np.float32)
+
+
+def training_pairs(sites: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """(features, targets, certified rank) of every non-buried site of one site set, from the
+    plain construction with K = 16 and one kNN step."""
+    algo = AlgorithmGPU(sites)
+    algo.build()
+    f = features(algo)
+    status = algo.debug_array("status")
+    _, _, ck = algo.contribution_profile(steps=1)
+    algo.close()
+    keep = status != 0xFF
+    return f[keep], labels(ck[keep]), ck[keep]
+
+
+def choose_margin(model: Model, features: np.ndarray, certified_k: np.ndarray, k: int = 16, check_cost: float = 1.0) -> float:
+    """Margin minimising the expected work of a cell on held-out data: neighbours inserted
+    (up to its proposal when it certifies there, all k otherwise) plus `check_cost` insertions
+    per failed early check."""
+    pred = model.predict(features).astype(np.float64)
+    ck = np.asarray(certified_k)
+    best, best_cost = 0.0, np.inf
+    for m in np.arange(-1.0, 2.01, 0.125):
+        r = np.clip(np.ceil(np.exp2(pred + m)), 1, k)
+        ok = (ck > 0) & (ck <= r)
+        cost = np.where(ok, r, k + np.where(r < k, check_cost, 0.0)).mean()
+        if cost < best_cost:
+            best, best_cost = float(m), float(cost)
+    return best

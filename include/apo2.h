@@ -119,6 +119,10 @@ typedef struct apo2_stats
     uint64_t device_bytes;         /* device memory held by the handle */
     uint32_t uncertified;          /* cells still in validation after the last round (APO2_ERR_ITER_LIMIT) */
     uint32_t reserved32;
+    uint64_t knn_insertions;       /* neighbours inserted by the kNN cell construction (all steps) */
+    uint64_t proposal_cells;       /* learned form: cells whose certificate was checked at a proposed rank */
+    uint64_t proposal_fallbacks;   /* ... of which failed there and went on through their list */
+    uint64_t proposal_skipped;     /* neighbours not inserted because the cell certified earlier */
 } apo2_stats;
 
 /* Library version string. */
@@ -195,6 +199,60 @@ apo2_status apo2_topology_json( apo2_handle * h, char * json, uint64_t capacity,
  * search walks the handle's BVH instead of all sites. */
 apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint32_t * ids, uint64_t count, uint32_t arity,
                           apo2_location location, uint8_t * flags, uint64_t * bad );
+
+/* Learned k-proposal (the north star's learned form; the reference only measures the labels,
+ * app/benchmarks/benchmark_contributing_nearest.cu:10-129). A 16 -> 64 -> 64 -> 1 network with
+ * ReLU, bf16 weights and fp32 accumulation predicts log2 of the kNN rank at which a site's cell
+ * passes the security-radius certificate, from 16 features of the site (radius, Morton-local
+ * density, radii and distances of its nearest neighbours; see apo2_proposal_features). With a
+ * model attached (apo2_set_proposal), the kNN kernel runs the network for every site and the kNN
+ * cell construction checks the certificate at the proposed rank ceil(2^(prediction + margin)):
+ * a cell that passes stops there (the later neighbours of its list cannot change a certified
+ * cell), one that does not goes on through the rest of its list as the plain method does (a
+ * fallback). Either way the certificate alone decides. */
+#define APO2_PROPOSAL_INPUTS 16
+#define APO2_PROPOSAL_HIDDEN 64
+#define APO2_PROPOSAL_PARAMS 5313 /* fp32 training vector: W1 (64 x 16), b1, W2 (64 x 64), b2, w3, b3 */
+
+typedef struct apo2_proposal
+{
+    uint32_t struct_size;                                         /* sizeof(apo2_proposal) */
+    uint32_t version;                                             /* 1 */
+    float    mean[ APO2_PROPOSAL_INPUTS ];                        /* inputs are (x - mean) * inv_scale */
+    float    inv_scale[ APO2_PROPOSAL_INPUTS ];
+    float    margin;                                              /* added to the prediction before 2^() */
+    float    b3;
+    float    b1[ APO2_PROPOSAL_HIDDEN ];
+    float    b2[ APO2_PROPOSAL_HIDDEN ];
+    uint16_t w1[ APO2_PROPOSAL_HIDDEN * APO2_PROPOSAL_INPUTS ];   /* bf16 bits, row-major (out x in) */
+    uint16_t w2[ APO2_PROPOSAL_HIDDEN * APO2_PROPOSAL_HIDDEN ];
+    uint16_t w3[ APO2_PROPOSAL_HIDDEN ];
+} apo2_proposal;
+
+/* Features of every site of a built handle, in sorted (Morton) order as apo2_debug_array:
+ * host float[16 * n]. */
+apo2_status apo2_proposal_features( apo2_handle * h, float * features );
+
+/* Predictions (log2 rank) of a model for n feature rows (host arrays). */
+apo2_status apo2_proposal_predict( const apo2_proposal * model, const float * features, uint64_t n, float * out );
+
+/* Mean squared error of one batch and its gradient with respect to the fp32 parameter vector
+ * `master` (APO2_PROPOSAL_PARAMS floats; the forward pass uses it rounded to bf16), computed by
+ * the training kernels; model supplies mean / inv_scale. For gradient checks. */
+apo2_status apo2_proposal_gradients( const apo2_proposal * model, const float * master, const float * features,
+                                     const float * targets, uint32_t n, float * loss, float * grads );
+
+/* Trains the network on the GPU (Adam, mean squared error on `targets`, batches of `batch`
+ * samples in a seeded random order each epoch). master: the fp32 parameter vector, initial on
+ * entry, trained on return; model: mean / inv_scale on entry, the bf16 weights and biases of the
+ * trained vector on return (margin untouched). epoch_loss (optional) receives each epoch's mean
+ * loss. All host arrays. */
+apo2_status apo2_proposal_train( const float * features, const float * targets, uint64_t n, uint32_t epochs, uint32_t batch,
+                                 float learning_rate, uint64_t seed, float * master, apo2_proposal * model, float * epoch_loss );
+
+/* Attaches a model to a handle (copied to the device): its next builds use the learned form.
+ * NULL detaches it (the plain form). */
+apo2_status apo2_set_proposal( apo2_handle * h, const apo2_proposal * model );
 
 /* Error of output vertices against an FP64 oracle, per result: each vertex (x, y, z, w) with its
  * four original site ids is refined by Newton steps on |p - c_a| - r_a - w = 0 (a = the four
@@ -330,6 +388,12 @@ apo2_status apo2_batch_create( uint32_t max_sites, uint32_t streams, const apo2_
 apo2_status apo2_batch_build( apo2_batch * b, const float * sites_xyzr, const uint64_t * site_offsets, uint32_t count,
                               uint64_t * vertex_offsets, double ** positions, uint32_t ** ids, float * build_ms );
 apo2_status apo2_batch_destroy( apo2_batch * b );
+
+/* Measured peak throughput of the FMA pipes of the current device, in TFLOP/s (2 FLOPs per fused
+ * multiply-add, many independent chains per thread, best of five launches): the denominators of
+ * the build's compute roofline, whose arithmetic is scalar FP64 and FP32. No counterpart in the
+ * reference. */
+apo2_status apo2_fma_peak( double * fp64_tflops, double * fp32_tflops );
 
 /* Seeded protein-like site set (host): `chains` self-avoiding random-walk chains of
  * `atoms_per_chain` atoms (bond 1.53 A, bond angle 109.5 +/- 10 deg, uniform torsion, van der

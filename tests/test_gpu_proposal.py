@@ -1,0 +1,148 @@
+"""Learned k-proposal: the GPU network, its training kernels and the learned build form.
+
+- features of the GPU match a numpy restatement of their definition;
+- predictions and the training kernels' loss and gradients match the CPU oracle
+  (oracle/mlp_oracle.py, float64 from the same bf16 weights) within GRAD_RTOL;
+- GPU training lowers the loss;
+- the learned form builds exactly the plain form's diagram (every store, status and output
+  array bit-identical), and the trained network inserts fewer neighbours than the method
+  without it (the plain form) and than an untrained network's proposals.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# fp32 accumulation over a batch of 2,000 against float64: relative to the largest gradient
+GRAD_RTOL = 2e-4
+PRED_ATOL = 2e-4
+FEATURE_ATOL = 2e-4
+
+
+@pytest.fixture(scope="module")
+def P():
+    import apo_b200
+    apo_b200.load_library()
+    from apo_b200 import proposal
+    return proposal
+
+
+def _random_batch(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(0, 1, (n, 16)).astype(np.float32) * rng.uniform(0.5, 3, 16).astype(np.float32) + 0.3
+    y = rng.uniform(0, 5, n).astype(np.float32)
+    return x, y
+
+
+def test_gradients_match_oracle(P):
+    from oracle import mlp_oracle as M
+    x, y = _random_batch(2000, 1)
+    model = P.Model.initial(x, seed=3)
+    # non-zero biases so every parameter group is exercised
+    rng = np.random.default_rng(4)
+    model.master = (model.master + rng.normal(0, 0.05, model.master.size)).astype(np.float32)
+    loss, g = model.gradients(x, y)
+    xn = M.normalise(x, model.mean, model.inv_scale)
+    ref_loss, ref_g = M.loss_and_gradients(model.master, xn, y)
+    assert abs(loss - ref_loss) <= 1e-4 * max(1.0, ref_loss)
+    scale = np.abs(ref_g).max()
+    assert np.max(np.abs(g - ref_g)) <= GRAD_RTOL * scale, np.max(np.abs(g - ref_g)) / scale
+
+
+def test_predictions_match_oracle(P):
+    from oracle import mlp_oracle as M
+    x, _ = _random_batch(5000, 2)
+    model = P.Model.initial(x, seed=5)
+    pred = model.predict(x)
+    ref, _ = M.forward(model.master, M.normalise(x, model.mean, model.inv_scale))
+    assert np.max(np.abs(pred - ref)) <= PRED_ATOL * max(1.0, np.abs(ref).max())
+
+
+def test_training_lowers_the_loss(P):
+    x, _ = _random_batch(20000, 3)
+    y = (0.5 * x[:, 0] - 0.25 * x[:, 3] + 0.1 * x[:, 5] ** 2 + 2.0).astype(np.float32)
+    model = P.Model.initial(x, seed=6)
+    losses = model.train(x, y, epochs=6, batch=1000, lr=3e-3)
+    assert losses[-1] < 0.25 * losses[0], losses
+    again = P.Model.initial(x, seed=6)
+    assert np.array_equal(again.train(x, y, epochs=6, batch=1000, lr=3e-3), losses)  # reproducible
+
+
+def _numpy_features(algo, n):
+    pos = algo.debug_array("sites_sorted").reshape(-1, 4)[:n].astype(np.float32)
+    knn = algo.debug_array("knn").reshape(n, -1)
+    codes = algo.debug_array("morton").astype(np.uint64)
+    sites = algo._sites.astype(np.float64)
+    lo = (sites[:, :3] - sites[:, 3:]).min(axis=0)
+    hi = (sites[:, :3] + sites[:, 3:]).max(axis=0)
+    scale = (np.float32(1.0) / (hi.astype(np.float32) - lo.astype(np.float32))).astype(np.float32)
+    out = np.zeros((n, 16), np.float64)
+    for i in range(n):
+        nb = [j for j in knn[i, :8] if j < n]
+        d = np.array([np.linalg.norm(pos[j, :3].astype(np.float64) - pos[i, :3]) for j in nb])
+        lam = d.mean() if len(nb) else max(pos[i, 3], 1e-3)
+        out[i, 0] = np.log2(pos[i, 3] / lam)
+        a, b = max(0, i - 16), min(n - 1, i + 16)
+        x = int(codes[a]) ^ int(codes[b])
+        level = (x.bit_length() - 1) // 3 + 1 if x else 0
+        log_volume = 3 * level - np.log2(scale.astype(np.float64)).sum() - 3 * np.log2(1048575.0)
+        out[i, 1] = np.log2(b - a + 1) + 3 * np.log2(lam) - log_volume
+        for q in range(7):
+            if q < len(nb):
+                j = nb[q]
+                out[i, 2 + q] = np.log2(pos[j, 3] / pos[i, 3])
+                out[i, 9 + q] = (d[q] - pos[i, 3] - pos[j, 3]) / lam
+            else:
+                out[i, 2 + q], out[i, 9 + q] = 0.0, 4.0
+    return out
+
+
+def test_features_match_their_definition(P):
+    import apo_b200
+    from apo_b200 import generators as g
+    sites = g.lognormal_cloud(3000, 40.0, seed=8)
+    algo = apo_b200.AlgorithmGPU(sites)
+    algo.build()
+    f = P.features(algo)
+    ref = _numpy_features(algo, sites.shape[0])
+    assert np.max(np.abs(f - ref) / np.maximum(1.0, np.abs(ref))) <= FEATURE_ATOL
+    algo.close()
+
+
+def _build(apo, sites, model):
+    from apo_b200 import proposal as P
+    algo = apo.AlgorithmGPU(sites)
+    if model is not None:
+        P.attach(algo, model)
+    algo.build()
+    return algo
+
+
+@pytest.mark.parametrize("kind", ["lognormal", "protein"])
+def test_learned_form_builds_the_plain_diagram_with_fewer_insertions(P, kind):
+    import apo_b200
+    from apo_b200 import generators as g
+    sites = (g.lognormal_cloud(60000, 400.0 * (60000 / 5e6) ** (1 / 3), seed=31) if kind == "lognormal"
+             else g.protein_chains(120, 500, 0.01, seed=32))
+    model = P.Model.load()
+    plain = _build(apo_b200, sites, None)
+    learned = _build(apo_b200, sites, model)
+    for name in ("status", "knn", "known_radii", "vertex_nb", "edge_nb", "vertices", "edges"):
+        assert np.array_equal(learned.debug_array(name), plain.debug_array(name)), name
+    a, b = learned.toHostFull(True), plain.toHostFull(True)
+    assert np.array_equal(a.verticesId, b.verticesId)
+    assert np.array_equal(a.vertices, b.vertices)
+    assert np.array_equal(a.closedEdgesId, b.closedEdgesId)
+    sp, sl = plain.stats(), learned.stats()
+    assert sp["proposal_cells"] == 0 and sl["proposal_cells"] > 0
+    assert sl["proposal_skipped"] > 0
+    # what the trained network gains over the method without it
+    assert sl["knn_insertions"] + sl["proposal_skipped"] == sp["knn_insertions"]
+    assert sl["knn_insertions"] < sp["knn_insertions"]
+    # ... and over an untrained network (He-initialised, no margin search)
+    untrained = P.Model.initial(P.features(plain), seed=99)
+    rough = _build(apo_b200, sites, untrained)
+    assert np.array_equal(rough.debug_array("vertices"), plain.debug_array("vertices"))
+    assert sl["knn_insertions"] + sl["proposal_fallbacks"] < rough.stats()["knn_insertions"] + rough.stats()["proposal_fallbacks"]
+    for x in (plain, learned, rough):
+        x.close()
