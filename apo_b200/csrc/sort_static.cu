@@ -2,14 +2,13 @@
 // working in scratch memory that the library reserves at load time instead of scratch the
 // caller allocates.
 //
-// Some callers cannot allocate device memory at the point where they sort: code recording a
-// CUDA graph that must contain no allocation nodes, latency-critical paths where cudaMalloc's
-// implicit synchronisation would stall other streams, and processes whose device memory is
-// owned by another allocator (a framework's caching allocator) that forbids foreign
-// allocations. They pass only the keys and values; the scratch -- the ping-pong copies, the
-// digit histograms, the look-back flags, the tile counters and an error word -- lives in a
-// file-scope __device__ array of fixed size, so every GPU that loads this library holds it
-// (kStaticSortBytes, about 12.3 MiB) until the process exits.
+// Some callers cannot allocate device memory at the point where they sort: processes whose
+// device memory is owned by another allocator (a framework's caching allocator) that forbids
+// foreign allocations, and latency-critical paths where cudaMalloc's implicit synchronisation
+// would stall other streams. They pass only the keys and values; the scratch -- the ping-pong
+// copies, the digit histograms, the look-back flags, the tile counters and an error word --
+// lives in a file-scope __device__ array of fixed size, so every GPU that loads this library
+// holds it (kStaticSortBytes, about 12.3 MiB) until the process exits.
 //
 // Limits and sharing:
 //   - at most kStaticSortPairs = 2^20 pairs per call; larger sizes are rejected;
@@ -19,8 +18,9 @@
 //     calls that overlap on the GPU (other streams, other host threads) race and corrupt
 //     each other's results;
 //   - the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call before any
-//     stream capture begins.
+//     (cudaGetSymbolAddress) with that device current;
+//   - a look-back wait that runs out is recounted exactly inside the sort; the error word
+//     that records it stays in the array and is not reported by this entry point.
 #include <cstdint>
 #include <mutex>
 

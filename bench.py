@@ -1,19 +1,25 @@
 """Benchmark of the Apollonius-diagram build on B200 (one JSON line on rank 0).
 
-Step = one complete diagram of the workload: LBVH, kNN, cell construction, the validation
-passes and the device-side extraction of the owned vertices and closed edges.
+Step = one complete diagram of the workload: LBVH, kNN (with the learned k-proposal's fused
+inference in the learned form), cell construction, the validation passes and the device-side
+extraction of the owned vertices and closed edges.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload protein1m] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload lognormal5m] [--form learned]
+                    [--impl reference]
 
-Workload (default): the protein-like packing of 1,000,000 sites (2,000 self-avoiding chains of
-500 atoms at 0.01 atoms/A^3, seed 1), float32 (x, y, z, r). Sites stay resident in HBM for
-`value`; `e2e` goes through the public API with pinned host buffers each step (upload of the
-sites, build, extraction, download of the vertices). Multi-GPU runs are independent replicas
-(one diagram per rank; the build does not shard), so scaling is weak.
+Workload (default): the 5,000,000-site evaluation cloud of the learned form -- centres uniform in
+[0, 400]^3, radii log-normal(0, 0.5) clipped to [0.2, 3.0], float32 (x, y, z, r), seed 7 (numpy).
+`value` is the headline form (--form, default the learned k-proposal) with the sites resident in
+HBM; the plain form is timed beside it on the same handle and the line says whether both built
+the same diagram. `e2e` goes through the public API with pinned host buffers each step (upload
+of the sites, build, extraction, download of the vertices). Multi-GPU runs are independent
+replicas (one diagram per rank), or with --shard one diagram split by Morton ranges of cells.
 
 --impl reference times the reference's CPU-side counterpart: the reference library has no CPU
 implementation of the path, so this is the project's CPU restatement of it (oracle/, all host
-threads) on a bounded sample of the workload.
+threads) on a bounded central sub-cube of the same workload; that arm also times the reference's
+own CUDA build (oracle/_ref, built from its sources) on the same workload, outside its timed
+region, when that binary is present.
 """
 from __future__ import annotations
 
@@ -33,6 +39,8 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 METRIC = "sites/sec full diagram (learned-k+FP32 vs plain) at identical topology, 1 B200"
+# forms of the build the line can time (the headline is --form)
+FORMS = ("plain", "learned")
 UNIT = "sites/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
@@ -44,7 +52,7 @@ C_QUAD = 216
 C_TEST = 11
 
 # DRAM bytes (read + write) per site of one build, by kernel, from one ncu capture of the
-# protein-like packing at 100,000 sites (profiles/top_kernels_protein100k.md), scaled by the
+# protein-like packing at 100,000 sites (--set full, one kernel per capture), scaled by the
 # sites processed.
 TRAFFIC_BYTES_PER_SITE = {"k_vertex_validation": 1839.3, "k_edge_speculate": 1536.5, "k_cells": 316.6,
                           "k_bisector_validation": 1054.6}
@@ -87,8 +95,10 @@ def workload(name: str, sites: int | None):
         return g.uniform_small(), {"workload": "uniform 10k (getUniform 10000, 100, 1.5, 0.5)", "sites": 10000}
     if name == "lognormal5m":
         n = sites or 5_000_000
-        return g.lognormal_cloud(n, 400.0 * (n / 5e6) ** (1 / 3), seed=7), {
-            "workload": "log-normal radii, uniform centres", "sites": n, "seed": 7}
+        side = 400.0 * (n / 5e6) ** (1 / 3)
+        return g.lognormal_cloud(n, side, seed=7), {
+            "workload": "log-normal radii, uniform centres (evaluation cloud of the learned form)", "sites": n,
+            "cube_side_A": round(side, 3), "radii": "log-normal(0, 0.5) clipped to [0.2, 3.0]", "seed": 7}
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -290,7 +300,7 @@ def run_reference(args, world, rank):
         print(json.dumps(line), flush=True)
         return
     sites, cfg = workload(args.workload, args.sites)
-    sample = min(args.cpu_sample, sites.shape[0])
+    sample = min(args.ref_sample, sites.shape[0])
     for _ in range(args.warmup):
         cpu_sample(sites, min(sample, 2000))
     times = []
@@ -302,13 +312,78 @@ def run_reference(args, world, rank):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(cfg, sample_sites=sample, note="reference has no CPU path; CPU restatement of it (oracle/)"),
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+        "note": "the reference has no CPU implementation of the path; CPU restatement of it (oracle/), all host "
+                "threads, each step a central sub-cube of the workload at its own density",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port",
                          "sample": f"{sample} sites of the workload (central sub-cube, same density), full diagram per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": reference_gpu_time(sites, args.ref_gpu_timeout),
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_time(sites: np.ndarray, timeout_s: float) -> dict:
+    """The reference's own CUDA build (its sources compiled by oracle/ref_build.sh) on the same
+    sites: constructor + build() timed by the reference driver with CUDA events (the region of
+    app/benchmarks/benchmark.cu:9-22). Outside every timed region of this arm."""
+    import tempfile
+    driver = os.path.join(ROOT, "oracle", "_ref", "apo_ref_driver")
+    if not os.path.exists(driver):
+        return {"status": "unavailable: the reference build (oracle/_ref) is absent"}
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "sites.f32")
+        np.ascontiguousarray(sites, dtype=np.float32).tofile(path)
+        t0 = time.perf_counter()
+        try:
+            run = subprocess.run([driver, path, tmp, "--time", "1", "--warmup", "0", "--no-dump"], capture_output=True, text=True,
+                                 timeout=timeout_s)
+        except subprocess.TimeoutExpired:
+            return {"status": f"did not finish within {timeout_s:.0f} s", "sites": int(sites.shape[0])}
+        wall = time.perf_counter() - t0
+        if run.returncode != 0:
+            return {"status": f"failed (exit {run.returncode})", "stderr": run.stderr[-300:]}
+        try:
+            meta = json.loads(run.stdout.strip().splitlines()[-1])
+        except (ValueError, IndexError):
+            return {"status": "unreadable driver output", "stdout": run.stdout[-300:]}
+    ms = meta.get("build_ms_median")
+    out = {"status": "ok", "sites": int(sites.shape[0]), "driver_wall_s": round(wall, 1), "driver": meta}
+    if ms:
+        out["ms"] = ms
+        out["sites_per_s"] = sites.shape[0] / (float(ms) / 1e3)
+    return out
+
+
+def _sha(a) -> str:
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def output_digest(algo) -> dict:
+    """Digests of the output and of the per-cell stores of the last build (form comparison)."""
+    v = algo.toHostFull(True)
+    return {"vertices_id": _sha(v.verticesId), "vertices": _sha(v.vertices), "closed_id": _sha(v.closedEdgesId),
+            "stores": _sha(algo.debug_array("vertices")) + _sha(algo.debug_array("edges")),
+            "status": _sha(algo.debug_array("status"))}
+
+
+def time_builds(algo, steps: int, world: int, stream: int = 0, clocks=None) -> float:
+    """Device time (CUDA events on the launching stream, the legacy default stream here) of
+    `steps` builds + extractions of a warmed-up handle, bracketed by a barrier and a
+    synchronisation on both sides; ms per step."""
+    import torch
+    torch.cuda.synchronize()
+    barrier(world)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(steps):
+        algo.build_and_extract(stream)
+    stop.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    return start.elapsed_time(stop) / steps
 
 
 def run_ours(args, world, rank, local):
@@ -317,53 +392,79 @@ def run_ours(args, world, rank, local):
     import torch
 
     import apo_b200
+    from apo_b200 import proposal
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     lib = apo_b200.load_library(build_if_missing=False)
     sites, cfg = workload(args.workload, args.sites)
     n = sites.shape[0]
     peaks, peaks_kind = load_peaks()
+    if not os.path.exists(proposal.DEFAULT_MODEL):
+        raise SystemExit(f"the trained k-proposal {proposal.DEFAULT_MODEL} is missing (apo_b200/models/train_proposal.py)")
+    model = proposal.Model.load()
 
-    # --- device-resident build (value) ---
+    def use_form(algo, form):
+        proposal.attach(algo, model if form == "learned" else None)
+
+    # --- device-resident builds (value): the headline form, then the plain form on the same handle ---
     # --shard: one diagram split over the ranks (each builds one Morton range of cells)
     shard = (rank, world) if args.shard else (0, 1)
     algo = apo_b200.AlgorithmGPU(sites, device=local, stage_timing=False, shard=shard)
     stream = 0  # legacy default stream: every launch and event below is on it
+    use_form(algo, args.form)
     for _ in range(args.warmup):
         algo.build_and_extract(stream)
         algo.output_counts()
-    stats = algo.stats()
-    launches = stats["kernel_launches"]
-    vcount, ccount = algo.output_counts()
-    torch.cuda.synchronize()
-    barrier(world)
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = algo.stats()["kernel_launches"]
     with ClockSampler(local) as clocks:
-        torch.cuda.synchronize()
-        start.record()
-        for _ in range(args.steps):
-            algo.build_and_extract(stream)
-        stop.record()
-        torch.cuda.synchronize()
-    barrier(world)
-    ms = start.elapsed_time(stop) / args.steps
+        ms = time_builds(algo, args.steps, world, stream)
     value, ms_max = (shard_rate if args.shard else aggregate_rate)(n, ms, world, device)
-    err = algo.stats()["error_flags"]
+    vcount, ccount = algo.output_counts()
+    stats = algo.stats()
+    digest = output_digest(algo)
     # interval certificate of every output vertex (the reference's precision check, on the GPU)
     t_c = time.perf_counter()
     bad_vertices, _ = algo.certify()
     certificate = {"vertices": int(vcount), "bad": int(bad_vertices), "seconds": round(time.perf_counter() - t_c, 3)}
+    # error of every output vertex against a Newton-refined IEEE double solve (per result)
+    mx, above, singular, errs = algo.vertex_error(threshold=1e-5)
+    vertex_error = {"max_rel": mx, "above_1e-5": int(above), "singular": int(singular),
+                    "p99_rel": float(np.percentile(errs, 99)) if errs.size else 0.0,
+                    "oracle": "Newton-refined IEEE double solve of each vertex's four sites"}
+
+    forms = {args.form: {"sites_per_s": value, "ms_per_step": ms_max, "steps": args.steps,
+                         "knn_insertions": int(stats["knn_insertions"]),
+                         "proposal_cells": int(stats["proposal_cells"]),
+                         "proposal_fallbacks": int(stats["proposal_fallbacks"]),
+                         "proposal_skipped": int(stats["proposal_skipped"])}}
+    for other in FORMS:
+        if other == args.form:
+            continue
+        use_form(algo, other)
+        algo.build_and_extract(stream)
+        algo.output_counts()
+        k2 = max(1, min(args.steps, 3))
+        ms2 = time_builds(algo, k2, world, stream)
+        v2, ms2_max = (shard_rate if args.shard else aggregate_rate)(n, ms2, world, device)
+        st2 = algo.stats()
+        forms[other] = {"sites_per_s": v2, "ms_per_step": ms2_max, "steps": k2,
+                        "knn_insertions": int(st2["knn_insertions"]),
+                        "identical_output": output_digest(algo) == digest}
+    use_form(algo, args.form)
+    learned = forms.get("learned", {})
+    if learned.get("proposal_cells"):
+        learned["fallback_rate"] = learned["proposal_fallbacks"] / learned["proposal_cells"]
+        learned["insertions_saved"] = learned["proposal_skipped"] / max(1, learned["knn_insertions"] + learned["proposal_skipped"])
 
     # --- per-kernel times of one more build (events around every launch) ---
     prof_algo = apo_b200.AlgorithmGPU(sites, device=local, stage_timing=True, shard=shard)
+    use_form(prof_algo, args.form)
     prof_algo.build_and_extract(stream)
     prof_algo.output_counts()
     prof = prof_algo.kernel_profile()
-    prof_stats = prof_algo.stats()
     prof_algo.close()
     kernels = prof["kernels"]
-    dominant = max(kernels.items(), key=lambda kv: kv[1][1])
-    dom_name, (dom_count, dom_ms) = dominant
+    dom_name, (dom_count, dom_ms) = max(kernels.items(), key=lambda kv: kv[1][1])
     total_ms = sum(v[1] for v in kernels.values())
 
     # algorithmic bytes (per diagram): sites read, vertices (position + ids) written, per-cell
@@ -374,7 +475,7 @@ def run_ours(args, world, rank, local):
     # algorithmic FP64 work (per diagram): every vertex is solved by its 4 cells and tested
     # against K neighbours -- 4 Q (C_QUAD + K C_TEST)
     f_alg = 4 * q * (C_QUAD + 16 * C_TEST)
-    fp64_peak = measure_fp64_peak(device)
+    fp64_peak, fp32_peak = apo_b200.fma_peak()
     dom_bytes_per_launch = b_alg * (dom_ms / total_ms) / max(1, dom_count)
     dom_avg_ms = dom_ms / max(1, dom_count)
     achieved = dom_bytes_per_launch / (dom_avg_ms / 1e3) / 1e9
@@ -383,17 +484,17 @@ def run_ours(args, world, rank, local):
         "frac": achieved / peaks["hbm_gbs"],
         "traffic": (TRAFFIC_BYTES_PER_SITE[dom_name] * n / max(1, dom_count)
                     if dom_name in TRAFFIC_BYTES_PER_SITE else None),
-        "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, from a 100k-site capture "
-                        "scaled by sites", "peak_kind": peaks_kind,
+        "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch from a 100k-site protein "
+                        "capture, scaled by sites", "peak_kind": peaks_kind,
         "kernel_share": dom_ms / total_ms, "kernel_avg_launch_ms": dom_avg_ms, "kernel_launches": dom_count,
         "algorithmic_bytes_per_diagram": b_alg,
-        "note": "path is FP64- and latency-bound (BVH walks, warp-collective cell updates), not HBM-bound; "
-                "see profiles/ for FP64 pipe and DRAM counters",
+        "note": "the path is latency-bound (dependent BVH-node and site loads in divergent walks, warp-collective "
+                "cell updates): neither HBM nor the FP64 pipe is the binding roof; both fractions are reported",
         "build_algorithmic_gbs": b_alg / (ms_max / 1e3) / 1e9,
         "fp64": {"achieved": f_alg / (ms_max / 1e3) / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
                  "frac": f_alg / (ms_max / 1e3) / 1e12 / fp64_peak if fp64_peak else None,
                  "algorithmic_flop_per_diagram": f_alg, "c_quad": C_QUAD, "c_test": C_TEST,
-                 "peak_kind": "measured here: cuBLAS DGEMM 4096^3 through torch, best of 5"},
+                 "peak_kind": "measured here: FMA-pipe microbenchmark (apo2_fma_peak)", "fp32_peak": fp32_peak},
     }
 
     # --- end to end through the public API with host buffers ---
@@ -425,7 +526,7 @@ def run_ours(args, world, rank, local):
     e2e_value, e2e_ms = (shard_rate if args.shard else aggregate_rate)(n, e0.elapsed_time(e1) / e2e_steps, world, device)
     d2h_job = reduce_sum(48.0 * written.value, world, device)
     e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(16 * n * world),
-           "d2h_bytes_per_step": int(d2h_job), "ms_per_step": e2e_ms, "steps": e2e_steps,
+           "d2h_bytes_per_step": int(d2h_job), "ms_per_step": e2e_ms, "steps": e2e_steps, "form": args.form,
            "bytes": "whole job: every rank uploads all sites and downloads its vertices"}
     vertices_job = int(reduce_sum(float(vcount), world, device)) if args.shard else int(vcount)
     algo.close()
@@ -440,18 +541,22 @@ def run_ours(args, world, rank, local):
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{got} sites of the workload (central sub-cube, same density), full diagram, {secs:.1f} s"}
 
+    plain = forms.get("plain", {})
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "strong" if args.shard else "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(cfg, form="plain (FP64 solves, reference topology)",
-                       parallelism=f"shards{world}" if args.shard else f"replicas{world}",
-                       l2="per-cell stores of several GB per diagram are rewritten every step (inputs >> 126 MB L2)",
-                       vertices=vertices_job, closed_edges=int(ccount), error_flags=int(err),
-                       validation_rounds=int(stats["validation_rounds"])),
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+        "form": {"plain": "plain (FP64 solves, K = 16)",
+                 "learned": "learned k-proposal (FP64 solves; no FP32 filter)"}[args.form],
+        "forms": forms,
+        "speedup_vs_plain": (value / plain["sites_per_s"]) if plain.get("sites_per_s") and args.form != "plain" else None,
+        "run": {"parallelism": f"shards{world}" if args.shard else f"replicas{world}",
+                "l2": "per-cell stores of tens of GB per diagram are rewritten every step (inputs >> 126 MB L2)",
+                "vertices": vertices_job, "closed_edges": int(ccount), "error_flags": int(stats["error_flags"]),
+                "validation_rounds": int(stats["validation_rounds"]), "uncertified": int(stats["uncertified"])},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(), "gpu_launches": launches * args.steps,
-        "certificate": certificate,
-        "kernel_ms": {k: round(v[1], 3) for k, v in sorted(kernels.items(), key=lambda kv: -kv[1][1])[:8]},
+        "certificate": certificate, "vertex_error": vertex_error,
+        "kernel_ms": {k: round(v[1], 3) for k, v in sorted(kernels.items(), key=lambda kv: -kv[1][1])[:10]},
     }
     print(json.dumps(line), flush=True)
 
@@ -665,9 +770,13 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="protein1m")
+    ap.add_argument("--workload", default="lognormal5m")
+    ap.add_argument("--form", default="learned", choices=FORMS, help="headline form of `value`")
     ap.add_argument("--sites", type=int, default=None)
-    ap.add_argument("--cpu-sample", type=int, default=100000)
+    ap.add_argument("--cpu-sample", type=int, default=30000, help="sites of the CPU baseline leg")
+    ap.add_argument("--ref-sample", type=int, default=15000, help="sites per step of the reference arm")
+    ap.add_argument("--ref-gpu-timeout", type=float, default=900.0,
+                    help="seconds allowed to the reference's own CUDA build in the reference arm")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--sets", type=int, default=4096, help="batch workload: number of site sets")
     ap.add_argument("--streams", type=int, default=8, help="batch workload: concurrent workers")

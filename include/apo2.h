@@ -362,13 +362,13 @@ apo2_status apo2_lbvh_build( const float * sites_xyzr, uint32_t n, const float s
 uint64_t    apo2_radix_sort_scratch_bytes( uint32_t n );
 apo2_status apo2_radix_sort_pairs( uint64_t * keys, uint32_t * values, uint32_t n, void * scratch, void * stream );
 
-/* The same sort for callers that cannot allocate device memory where they sort (a graph
- * recording that must hold no allocation, a latency-critical path where cudaMalloc would
- * synchronise, memory owned by another allocator). No counterpart in the reference. Its
- * scratch is a fixed __device__ array of the library (about 12.3 MiB per GPU, held until
- * exit); at most 2^20 pairs, APO2_ERR_TOO_LARGE above. All calls on a device share that
- * array, so calls that overlap on the GPU race; calls in sequence are independent. The
- * first call on a device looks the array up and should come before any stream capture. */
+/* The same sort for callers that cannot allocate device memory where they sort (memory owned by
+ * another allocator, a latency-critical path where cudaMalloc would synchronise). No counterpart
+ * in the reference. Its scratch is a fixed __device__ array of the library (about 12.3 MiB per GPU,
+ * held until exit); at most 2^20 pairs, APO2_ERR_TOO_LARGE above. All calls on a device share
+ * that array, so calls that overlap on the GPU race; calls in sequence are independent. The first
+ * call on a device looks the array up with that device current. A look-back wait that runs out is
+ * recounted exactly (see apo2_radix_sort_pairs); this entry point does not report it. */
 apo2_status apo2_radix_sort_pairs_static( uint64_t * keys, uint32_t * values, uint32_t n, void * stream );
 
 /* Batched form: many independent diagrams of uneven size in one call (the reference builds one

@@ -202,7 +202,7 @@ struct StagedBuild : apo::gpu::AlgorithmGPU<K>
 
 template<uint32_t K>
 void runReference( std::vector<apo::Real> & sites, const uint32_t n, const std::string & outDir, const int repeat,
-                   const bool dump, const uint32_t knnSteps, std::string & json )
+                   const bool dump, const uint32_t knnSteps, std::string & json, const int warmup = 3 )
 {
 
     if ( repeat > 0 )
@@ -212,7 +212,7 @@ void runReference( std::vector<apo::Real> & sites, const uint32_t n, const std::
         cudaEventCreate( &stop );
         std::vector<float> times;
         double stage[ 7 ] = { 0, 0, 0, 0, 0, 0, 0 };
-        for ( int r = -3; r < repeat; r++ )
+        for ( int r = -warmup; r < repeat; r++ )
         {
             cudaDeviceSynchronize();
             cudaEventRecord( start );
@@ -350,12 +350,13 @@ int main( int argc, char ** argv )
 {
     if ( argc < 3 )
     {
-        std::fprintf( stderr, "usage: %s sites.f32 outdir [--time R] [--no-dump] [--k 1|4|8|16] [--knn-steps S] [--stages]\n", argv[ 0 ] );
+        std::fprintf( stderr, "usage: %s sites.f32 outdir [--time R] [--warmup W] [--no-dump] [--k 1|4|8|16] [--knn-steps S] [--stages]\n", argv[ 0 ] );
         return 1;
     }
     const std::string input  = argv[ 1 ];
     const std::string outDir = argv[ 2 ];
     int               repeat = 0;
+    int               warmup = 3; // untimed builds before the timed ones
     bool              dump   = true;
     uint32_t          k        = 16; // AlgorithmGPU<K>
     uint32_t          knnSteps = 1;  // knnValidationStep
@@ -364,6 +365,8 @@ int main( int argc, char ** argv )
     {
         if ( !std::strcmp( argv[ a ], "--time" ) && a + 1 < argc )
             repeat = std::atoi( argv[ ++a ] );
+        else if ( !std::strcmp( argv[ a ], "--warmup" ) && a + 1 < argc )
+            warmup = std::max( 0, std::atoi( argv[ ++a ] ) );
         else if ( !std::strcmp( argv[ a ], "--no-dump" ) )
             dump = false;
         else if ( !std::strcmp( argv[ a ], "--k" ) && a + 1 < argc )
@@ -404,10 +407,10 @@ int main( int argc, char ** argv )
     }
     switch ( k )
     {
-    case 1: runReference<1>( sites, n, outDir, repeat, dump, knnSteps, json ); break;
-    case 4: runReference<4>( sites, n, outDir, repeat, dump, knnSteps, json ); break;
-    case 8: runReference<8>( sites, n, outDir, repeat, dump, knnSteps, json ); break;
-    case 16: runReference<16>( sites, n, outDir, repeat, dump, knnSteps, json ); break;
+    case 1: runReference<1>( sites, n, outDir, repeat, dump, knnSteps, json, warmup ); break;
+    case 4: runReference<4>( sites, n, outDir, repeat, dump, knnSteps, json, warmup ); break;
+    case 8: runReference<8>( sites, n, outDir, repeat, dump, knnSteps, json, warmup ); break;
+    case 16: runReference<16>( sites, n, outDir, repeat, dump, knnSteps, json, warmup ); break;
     default: std::fprintf( stderr, "k must be 1, 4, 8 or 16\n" ); return 1;
     }
 

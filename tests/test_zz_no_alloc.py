@@ -1,8 +1,8 @@
 """The sort entry point that allocates nothing (apo2_radix_sort_pairs_static).
 
-It serves callers that cannot allocate device memory where they sort, e.g. while recording a
-CUDA graph that must hold no allocation nodes, or under a memory owner that forbids other
-allocations: its scratch is a fixed array inside the library. This file is collected last
+It serves callers that cannot allocate device memory where they sort, e.g. under a memory
+owner that forbids other allocations, or where an allocation's implicit synchronisation would
+stall other work: its scratch is a fixed array inside the library. This file is collected last
 so that a stop at its first failure has already run every other test; it also passes alone
 in a fresh process. Integer sort: results must be identical to apo2_radix_sort_pairs.
 """
