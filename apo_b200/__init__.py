@@ -30,6 +30,7 @@ APO2_ERR_NOT_BUILT, APO2_ERR_OUT_OF_MEMORY, APO2_ERR_TOO_LARGE = 5, 6, 7
 APO2_F32, APO2_F64 = 0, 1
 APO2_HOST, APO2_DEVICE = 0, 1
 APO2_NO_KNN_STEPS = 0xFFFFFFFF
+APO2_PRECISION_FP64, APO2_PRECISION_FP32_FILTER = 0, 1
 
 _STATUS_NAMES = {
     0: "APO2_OK", 1: "APO2_ERR_INVALID_ARG", 2: "APO2_ERR_CAPACITY", 3: "APO2_ERR_ITER_LIMIT",
@@ -47,7 +48,8 @@ class Options(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("k", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32),
                 ("device", ctypes.c_uint32), ("stage_timing", ctypes.c_uint32), ("edge_search", ctypes.c_uint32),
                 ("knn_steps", ctypes.c_uint32), ("stop_after", ctypes.c_uint32), ("shard_index", ctypes.c_uint32),
-                ("shard_count", ctypes.c_uint32), ("wait_limit", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 5)]
+                ("shard_count", ctypes.c_uint32), ("wait_limit", ctypes.c_uint32), ("precision", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 4)]
 
 
 class Stats(ctypes.Structure):
@@ -60,7 +62,8 @@ class Stats(ctypes.Structure):
                 ("ms_edge_validation", ctypes.c_double), ("ms_bisector_validation", ctypes.c_double),
                 ("ms_output", ctypes.c_double), ("device_bytes", ctypes.c_uint64), ("uncertified", ctypes.c_uint32),
                 ("reserved32", ctypes.c_uint32), ("knn_insertions", ctypes.c_uint64), ("proposal_cells", ctypes.c_uint64),
-                ("proposal_fallbacks", ctypes.c_uint64), ("proposal_skipped", ctypes.c_uint64)]
+                ("proposal_fallbacks", ctypes.c_uint64), ("proposal_skipped", ctypes.c_uint64),
+                ("filter_tests", ctypes.c_uint64), ("filter_escalations", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("reserved")}
@@ -179,11 +182,13 @@ class AlgorithmGPU:
 
     def __init__(self, sites, knnValidationStep: int = 1, k: int = 16, max_iterations: int = 10, device: int = 0,
                  stage_timing: bool = False, edge_search: int = 0, stop_after: int = 0, shard: tuple[int, int] = (0, 1),
-                 wait_limit: int = 0):
+                 wait_limit: int = 0, precision: str = "fp64"):
         """`shard` = (index, count): build only the cells of one of `count` contiguous Morton
         ranges of the sites (one diagram over several GPUs); the shards' outputs, concatenated in
         shard order, are the whole diagram's. `wait_limit`: polls per look-back wait of the
-        LBVH's radix sort before a tile recounts its digits itself (0 = the library default)."""
+        LBVH's radix sort before a tile recounts its digits itself (0 = the library default).
+        `precision`: "fp64" (the plain form) or "fp32" (conflict predicates through the FP32
+        static filter, FP64 inside its bound; the same diagram)."""
         lib = load_library()
         self._sites, dtype = _as_sites(sites)
         self.n = int(self._sites.shape[0])
@@ -198,6 +203,7 @@ class AlgorithmGPU:
         opt.stop_after = stop_after
         opt.shard_index, opt.shard_count = int(shard[0]), int(shard[1])
         opt.wait_limit = int(wait_limit)
+        opt.precision = {"fp64": APO2_PRECISION_FP64, "fp32": APO2_PRECISION_FP32_FILTER}[precision]
         self.knnValidationStep = knnValidationStep
         self._k = k
         handle = ctypes.c_void_p()

@@ -461,6 +461,7 @@ namespace
         c.walk_scratch    = a.take<uint32_t>( walk_scratch_bytes() / sizeof( uint32_t ) );
         c.work_counter    = a.take<uint32_t>( 1 );
         c.counters        = a.take<unsigned long long>( kCounters );
+        c.fp32            = opt.precision == APO2_PRECISION_FP32_FILTER ? 1u : 0u;
         c.codes           = t.codes;
         sort_scratch_carve( h->sort, sortBase, n, h->error );
         return a.used <= a.size;
@@ -496,6 +497,8 @@ namespace
         opt.max_iterations = std::min( opt.max_iterations, kMaxRounds );
         if ( opt.shard_count == 0 )
             opt.shard_count = 1;
+        if ( opt.precision > APO2_PRECISION_FP32_FILTER )
+            return fail( APO2_ERR_INVALID_ARG, "precision is APO2_PRECISION_FP64 or APO2_PRECISION_FP32_FILTER" );
         if ( opt.shard_index >= opt.shard_count )
             return fail( APO2_ERR_INVALID_ARG, "shard_index must be below shard_count" );
         return APO2_OK;
@@ -1280,6 +1283,8 @@ apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
     s.proposal_cells     = cnt[ kCountChecked ];
     s.proposal_fallbacks = cnt[ kCountFallbacks ];
     s.proposal_skipped   = cnt[ kCountSkipped ];
+    s.filter_tests       = cnt[ kCountFiltered ];
+    s.filter_escalations = cnt[ kCountEscalated ];
     s.kernel_launches = h->launches;
     if ( h->timing )
     {

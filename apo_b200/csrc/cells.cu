@@ -61,6 +61,7 @@ namespace apo2
         double4 * pos;   // solved position of v[*]
         uint4 * e;       // (j, k, vertex count, status | validated << 8), capacity kEdgeSlots
         uint32_t vn, en; // warp-uniform sizes
+        mutable FilterTally tally; // this lane's FP32-filter counts
     };
 
     __device__ __forceinline__ uint32_t vstatus( uint4 r ) { return ( r.w >> 8 ) & 0xffu; }
@@ -83,9 +84,9 @@ namespace apo2
             {
                 const uint4 r = w.e[ e ];
                 if ( r.x != skip1 && r.x != skip2 )
-                    ok = ok && !intersects( site( c, r.x ), sphere );
+                    ok = ok && !site_conflict( c, r.x, sphere, w.tally );
                 if ( r.y != skip1 && r.y != skip2 )
-                    ok = ok && !intersects( site( c, r.y ), sphere );
+                    ok = ok && !site_conflict( c, r.y, sphere, w.tally );
             }
             if ( !__all_sync( kFull, ok ) )
                 return false;
@@ -116,9 +117,9 @@ namespace apo2
         for ( uint32_t e = 0; e < w.en; e++ )
         {
             const uint4 r = w.e[ e ];
-            if ( r.x != skip1 && r.x != skip2 && intersects( site( c, r.x ), sphere ) )
+            if ( r.x != skip1 && r.x != skip2 && site_conflict( c, r.x, sphere, w.tally ) )
                 return false;
-            if ( r.y != skip1 && r.y != skip2 && intersects( site( c, r.y ), sphere ) )
+            if ( r.y != skip1 && r.y != skip2 && site_conflict( c, r.y, sphere, w.tally ) )
                 return false;
         }
         return true;
@@ -257,7 +258,7 @@ namespace apo2
             bool           invalid = false;
             if ( id < baseV )
             {
-                invalid = intersects( w.pos[ id ], sj );
+                invalid = sphere_conflict( c, sj, w.pos[ id ], w.tally );
                 if ( invalid )
                     w.v[ id ].w |= 0xff00u;
             }
@@ -598,8 +599,9 @@ namespace apo2
         w.pos = reinterpret_cast<double4 *>( base );
         w.v   = reinterpret_cast<uint4 *>( base + sizeof( double4 ) * kVertexSlots );
         w.e   = reinterpret_cast<uint4 *>( base + ( sizeof( double4 ) + sizeof( uint4 ) ) * kVertexSlots );
-        w.vn  = 0;
-        w.en  = 0;
+        w.vn    = 0;
+        w.en    = 0;
+        w.tally = FilterTally {};
         return w;
     }
 
@@ -649,6 +651,21 @@ namespace apo2
         err = __reduce_or_sync( kFull, err );
         if ( err && lane_id() == 0 )
             atomicOr( c.error, err );
+    }
+    // Error flags and the FP32 filter's counts of a warp at the end of a kernel.
+    __device__ __forceinline__ void report( const CellContext & c, uint32_t err, const WarpCell & w )
+    {
+        report( c, err );
+        if ( c.fp32 && c.counters )
+        {
+            const uint32_t tests = __reduce_add_sync( kFull, w.tally.tests );
+            const uint32_t esc   = __reduce_add_sync( kFull, w.tally.escalated );
+            if ( lane_id() == 0 )
+            {
+                atomicAdd( c.counters + kCountFiltered, static_cast<unsigned long long>( tests ) );
+                atomicAdd( c.counters + kCountEscalated, static_cast<unsigned long long>( esc ) );
+            }
+        }
     }
 
     // -----------------------------------------------------------------------------------
@@ -962,7 +979,7 @@ namespace apo2
             store_cell( c, w, i, 0, err );
             __syncwarp();
         }
-        report( c, err );
+        report( c, err, w );
         __syncwarp();
         if ( c.counters && lane_id() == 0 )
             for ( uint32_t t = 0; t < kCounters; t++ )
@@ -1034,7 +1051,7 @@ namespace apo2
             store_cell( c, w, i, 0, err );
             __syncwarp();
         }
-        report( c, err );
+        report( c, err, w );
     }
 
     // -----------------------------------------------------------------------------------
@@ -1219,7 +1236,7 @@ namespace apo2
             store_cell( c, w, i, 0, err );
             __syncwarp();
         }
-        report( c, err );
+        report( c, err, w );
     }
 
     // -----------------------------------------------------------------------------------
@@ -1755,7 +1772,7 @@ namespace apo2
             store_cell( c, w, i, base, err );
             __syncwarp();
         }
-        report( c, err );
+        report( c, err, w );
     }
 
     // -----------------------------------------------------------------------------------
@@ -2020,7 +2037,7 @@ namespace apo2
             store_cell( c, w, i, base, err );
             __syncwarp();
         }
-        report( c, err );
+        report( c, err, w );
     }
 
     // -----------------------------------------------------------------------------------

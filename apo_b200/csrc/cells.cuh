@@ -48,10 +48,48 @@ namespace apo2
         const ProposalNet * proposal   = nullptr;
         const uint64_t *    codes      = nullptr;
         uint8_t *           proposed_k = nullptr;
-        // build counters: kNN insertions, cells checked at a proposed rank, fallbacks, skipped neighbours
+        // build counters: kNN insertions, cells checked at a proposed rank, fallbacks, skipped
+        // neighbours, conflict predicates decided by the FP32 filter, those it left to FP64
         unsigned long long * counters = nullptr;
+        // FP32-filtered form: conflict predicates against sites first in single precision
+        uint32_t fp32 = 0;
     };
-    constexpr uint32_t kCountInsertions = 0, kCountChecked = 1, kCountFallbacks = 2, kCountSkipped = 3, kCounters = 4;
+    constexpr uint32_t kCountInsertions = 0, kCountChecked = 1, kCountFallbacks = 2, kCountSkipped = 3, kCountFiltered = 4,
+                       kCountEscalated = 5, kCounters = 6;
+
+    // Lane-local tallies of the FP32 filter, added to the build's counters when a kernel ends.
+    struct FilterTally
+    {
+        uint32_t tests = 0, escalated = 0;
+    };
+
+    // The reference's conflict test of site `id` against the sphere x (gpu/math.cuh:374-388),
+    // decided by the FP32 filter where it can in the filtered form.
+    __device__ __forceinline__ bool site_conflict( const CellContext & c, uint32_t id, double4 x, FilterTally & t )
+    {
+        if ( c.fp32 )
+        {
+            t.tests++;
+            const int f = conflict_filter( c.sites_f[ id ], x );
+            if ( f != 2 )
+                return f == 1;
+            t.escalated++;
+        }
+        return intersects( c.sites[ id ], x );
+    }
+    // The same for a site given by value (its float copy is exact for float input and bounded otherwise).
+    __device__ __forceinline__ bool sphere_conflict( const CellContext & c, double4 site, double4 x, FilterTally & t )
+    {
+        if ( c.fp32 )
+        {
+            t.tests++;
+            const int f = conflict_filter( to_float( site ), x );
+            if ( f != 2 )
+                return f == 1;
+            t.escalated++;
+        }
+        return intersects( site, x );
+    }
 
     // Row of cell i in the per-cell stores (vertices, edges), which hold only the cells
     // [lo, hi) a handle builds: a shard of the diagram needs stores for its own cells alone.

@@ -265,6 +265,8 @@ namespace apo2
         const uint32_t mask   = quadrisector( s.si, sj, s.sk, s.sl, x[ 0 ], x[ 1 ] );
         if ( mask != 3 )
             return false;
+        // the FP32 filter decides here too; its counts are kept for the cell kernels only
+        FilterTally untallied;
         for ( uint32_t r = 0; r < 2; r++ )
         {
             bool ok = true;
@@ -272,7 +274,7 @@ namespace apo2
             {
                 const uint32_t u = s.nbr[ q ];
                 if ( u != s.k && u != s.l )
-                    ok = !intersects( c.sites[ u ], x[ r ] );
+                    ok = !site_conflict( c, u, x[ r ], untallied );
             }
             if ( ok )
                 return true;

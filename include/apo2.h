@@ -87,8 +87,16 @@ typedef struct apo2_options
                                       counts its digits itself (exact either way; 0 = 2^22). Tests set
                                       it small to exercise that path; apo2_stats.error_flags bit 32
                                       reports that a wait ran out */
-    uint32_t reserved[ 5 ];
+    uint32_t precision;            /* APO2_PRECISION_FP64 (0, the plain form) or APO2_PRECISION_FP32_FILTER:
+                                      conflict predicates against sites are first evaluated in single
+                                      precision from a float copy of the sites under a static error
+                                      bound, and only those inside the bound in the reference's FP64
+                                      arithmetic; every decision, and so the diagram, is the same */
+    uint32_t reserved[ 4 ];
 } apo2_options;
+
+#define APO2_PRECISION_FP64        0u
+#define APO2_PRECISION_FP32_FILTER 1u
 
 #define APO2_NO_KNN_STEPS 0xffffffffu
 
@@ -123,6 +131,8 @@ typedef struct apo2_stats
     uint64_t proposal_cells;       /* learned form: cells whose certificate was checked at a proposed rank */
     uint64_t proposal_fallbacks;   /* ... of which failed there and went on through their list */
     uint64_t proposal_skipped;     /* neighbours not inserted because the cell certified earlier */
+    uint64_t filter_tests;         /* FP32-filtered form: conflict predicates of the cell kernels */
+    uint64_t filter_escalations;   /* ... that fell inside the bound and were evaluated in FP64 */
 } apo2_stats;
 
 /* Library version string. */

@@ -1,0 +1,52 @@
+"""FP32-filtered form: the conflict predicates against sites are decided in single precision under
+a static error bound and escalated to the reference's FP64 arithmetic inside it, so every store,
+status and output array must stay bit-identical to the reference's dumps (the same bar as the
+plain form), while the filter decides most predicates by itself."""
+import numpy as np
+import pytest
+
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def apo():
+    import apo_b200
+    apo_b200.load_library()
+    return apo_b200
+
+
+@pytest.mark.parametrize("case", H.STORED_CASES + ["uni2k_s2", "prec2_k1s4"])
+def test_fp32_form_matches_reference_dump(apo, case):
+    golden = H.load_golden(case)
+    k, steps = H.case_params(case)
+    algo = apo.AlgorithmGPU(H.sites_for(case), knnValidationStep=steps, k=k, precision="fp32")
+    algo.build()
+    for name in H.exact_names(case):
+        if name.startswith("topo_"):
+            continue
+        assert np.array_equal(algo.debug_array(name), golden[name]), f"{case}: {name}"
+    full = algo.toHostFull(True)
+    assert np.array_equal(full.verticesId, golden["vertices_id"])
+    assert H.rel_err(full.vertices, golden["vertices_pos"]) <= 1e-9
+    st = algo.stats()
+    assert st["filter_tests"] > 0
+    algo.close()
+
+
+@pytest.mark.parametrize("case", ["uni100k", "logn50k", "protein100k", "latticeA20"])
+def test_fp32_form_matches_reference_digests(apo, case):
+    d = H.digests()[case]
+    algo = apo.AlgorithmGPU(H.sites_for(case), precision="fp32")
+    algo.build()
+    for name in ("indices", "status", "knn", "vertex_nb", "edge_nb", "vertices", "edges"):
+        assert H.sha(algo.debug_array(name)) == d["arrays"][name], f"{case}: {name}"
+    full = algo.toHostFull(True)
+    assert H.sha(full.verticesId) == d["arrays"]["vertices_id"]
+    st = algo.stats()
+    rate = st["filter_escalations"] / max(1, st["filter_tests"])
+    # the filter decides nearly everything on generic clouds; the tangent-sphere lattice puts
+    # many distances near zero on purpose
+    assert rate < (0.5 if case == "latticeA20" else 0.05), rate
+    algo.close()
