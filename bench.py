@@ -561,6 +561,20 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_once(args, local):
+    """Two builds of the workload with the --form form (profiling aid, nothing timed)."""
+    import apo_b200
+    from apo_b200 import proposal
+    sites, _ = workload(args.workload, args.sites)
+    algo = apo_b200.AlgorithmGPU(sites, device=local)
+    if args.form == "learned":
+        proposal.attach(algo, proposal.Model.load())
+    for _ in range(2):
+        algo.build_and_extract(0)
+        algo.output_counts()
+    algo.close()
+
+
 def batch_sets(count: int, lo: int, hi: int, seed: int = 3):
     """Protein-like site sets with sizes log-uniform in [lo, hi] (chains of 100 atoms at
     0.01 atoms/A^3, one seed per set)."""
@@ -780,12 +794,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--sets", type=int, default=4096, help="batch workload: number of site sets")
     ap.add_argument("--streams", type=int, default=8, help="batch workload: concurrent workers")
+    ap.add_argument("--once", action="store_true",
+                    help="profiling aid: build the workload's diagram twice with --form (a warm-up and one more) and exit, "
+                         "no timing and no JSON line (for an ncu launch list or a one-kernel capture)")
     ap.add_argument("--shard", action="store_true",
                     help="N>1: one diagram split over the ranks (Morton ranges of cells) instead of N replicas")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.once:
+            run_once(args, local)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         elif args.workload == "batch":
             run_batch(args, world, rank, local)

@@ -131,7 +131,7 @@ int main(int argc, char **) {
     // the cavity application's directions are computed on the host
     const std::vector<float> dirs = apo::gpu::getDirections(64);
     if (dirs.size() != 192 || dirs[0] != 0.f || dirs[1] != 0.f || dirs[2] != -1.f) return 3;
-    if (argc > 5) {  // never taken in the test: shows the reference's call sequence compiles
+    if (argc > 5) {  // not taken here: the call sequence runs on a GPU in tests/test_gpu_compat_cpp.py
         apo::gpu::CavityDetection cavity{span};
         std::vector<float> loaded(xyzr.begin(), xyzr.end());
         auto ratios = cavity.getHitRatios(apo::ConstSpan<float>{loaded});
