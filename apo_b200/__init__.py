@@ -112,6 +112,7 @@ SIGNATURES = {
     "apo2_batch_create": (_I, [_U32, _U32, _P, _P]),
     "apo2_batch_build": (_I, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "apo2_batch_destroy": (_I, [_P]),
+    "apo2_batch_set_proposal": (_I, [_P, _P]),
     "apo2_cavity_directions": (_I, [_U32, _P]),
     "apo2_cavity_hit_ratios": (_I, [_P, _P, _U32, _I, _U32, _P, _U64, _P, _P]),
     "apo2_cavity_vertices": (_I, [_P, ctypes.c_float, ctypes.c_float, _P, _U64, _P]),
@@ -388,16 +389,23 @@ class Batch:
     """Many independent diagrams of uneven size per call (apo2_batch_*): `streams` workers, each
     with device memory for `max_sites` sites, build the diagrams largest first, overlapping."""
 
-    def __init__(self, max_sites: int, streams: int = 8, k: int = 16, device: int = 0):
+    def __init__(self, max_sites: int, streams: int = 8, k: int = 16, device: int = 0, precision: str = "fp64",
+                 proposal=None):
+        """`precision` and `proposal` (an apo_b200.proposal.Model) select the forms, as for
+        AlgorithmGPU; every form builds the same diagrams."""
         lib = load_library()
         opt = Options()
         opt.struct_size = ctypes.sizeof(Options)
         opt.k = k
         opt.device = device
+        opt.precision = {"fp64": APO2_PRECISION_FP64, "fp32": APO2_PRECISION_FP32_FILTER}[precision]
         handle = ctypes.c_void_p()
         _check(lib.apo2_batch_create(max_sites, streams, ctypes.byref(opt), ctypes.byref(handle)))
         self._b = handle
         self._lib = lib
+        if proposal is not None:
+            p = proposal.struct()
+            _check(lib.apo2_batch_set_proposal(handle, ctypes.byref(p)))
 
     def build(self, diagrams, vertices: bool = True):
         """diagrams: list of (n_i, 4) float32 arrays. Returns (list of VertexDiagram or None,

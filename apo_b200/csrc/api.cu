@@ -1761,6 +1761,19 @@ apo2_status apo2_batch_build( apo2_batch * b, const float * sites_xyzr, const ui
     return APO2_OK;
 }
 
+apo2_status apo2_batch_set_proposal( apo2_batch * b, const apo2_proposal * model )
+{
+    if ( !b )
+        return fail( APO2_ERR_INVALID_ARG, "null batch" );
+    for ( auto & w : b->workers )
+    {
+        const apo2_status st = apo2_set_proposal( w.h, model );
+        if ( st != APO2_OK )
+            return st;
+    }
+    return APO2_OK;
+}
+
 apo2_status apo2_batch_destroy( apo2_batch * b )
 {
     destroy_batch( b );

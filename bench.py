@@ -611,7 +611,18 @@ def run_batch(args, world, rank, local):
             if args.shard and world > 1 else all_sets)
     if not sets:
         raise SystemExit("fewer site sets than ranks")
-    batch = apo_b200.Batch(max(int(d.shape[0]) for d in sets), streams=args.streams, device=local)
+    tuned = None
+    if args.autotune:
+        # the project's autotuner: workers, FP32 filter and learned proposal picked on a sample
+        # (every candidate builds the same diagrams)
+        from apo_b200 import autotune, proposal
+        model = proposal.Model.load() if os.path.exists(proposal.DEFAULT_MODEL) else None
+        tuned = autotune.autotune_batch(sets, proposal=model, device=local)
+        best = tuned["best"]
+        batch = apo_b200.Batch(max(int(d.shape[0]) for d in sets), streams=best["streams"], device=local,
+                               precision=best["precision"], proposal=model if best["learned"] else None)
+    else:
+        batch = apo_b200.Batch(max(int(d.shape[0]) for d in sets), streams=args.streams, device=local)
     for _ in range(args.warmup):
         batch.build(sets, vertices=False)
     torch.cuda.synchronize()
@@ -654,6 +665,7 @@ def run_batch(args, world, rank, local):
                    "parallelism": (f"sets split over {world} ranks" if args.shard else f"replicas{world}")},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "loop_of_single_builds": {"value": loop_rate, "unit": UNIT, "sets": min(256, len(sets))},
+        "autotune": tuned,
         "e2e": {"value": (1 if args.shard else world) * total / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": int(16 * total * (1 if args.shard else world)),
                 "d2h_bytes_per_step": int(48 * vertices * (1 if args.shard else world))},
@@ -794,6 +806,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--sets", type=int, default=4096, help="batch workload: number of site sets")
     ap.add_argument("--streams", type=int, default=8, help="batch workload: concurrent workers")
+    ap.add_argument("--autotune", action="store_true", help="batch workload: pick workers and forms by measurement first")
     ap.add_argument("--once", action="store_true",
                     help="profiling aid: build the workload's diagram twice with --form (a warm-up and one more) and exit, "
                          "no timing and no JSON line (for an ncu launch list or a one-kernel capture)")

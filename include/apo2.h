@@ -397,6 +397,8 @@ apo2_status apo2_batch_create( uint32_t max_sites, uint32_t streams, const apo2_
  * count floats) receives each diagram's device time from its upload to the end of its extraction. */
 apo2_status apo2_batch_build( apo2_batch * b, const float * sites_xyzr, const uint64_t * site_offsets, uint32_t count,
                               uint64_t * vertex_offsets, double ** positions, uint32_t ** ids, float * build_ms );
+/* Attaches a learned k-proposal to every worker of a batch (NULL: the plain form). */
+apo2_status apo2_batch_set_proposal( apo2_batch * b, const apo2_proposal * model );
 apo2_status apo2_batch_destroy( apo2_batch * b );
 
 /* Measured peak throughput of the FMA pipes of the current device, in TFLOP/s (2 FLOPs per fused
