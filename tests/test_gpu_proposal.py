@@ -109,6 +109,26 @@ def test_features_match_their_definition(P):
     algo.close()
 
 
+@pytest.fixture(scope="module")
+def model(P):
+    """The shipped model (apo_b200/models/proposal_k16.npz), or, where it is absent, one trained
+    here the same way on a few small diagrams."""
+    import os
+    if os.path.exists(P.DEFAULT_MODEL):
+        return P.Model.load()
+    from apo_b200 import generators as g
+    pairs = [P.training_pairs(s) for s in (g.lognormal_cloud(50000, 400.0 * (50000 / 5e6) ** (1 / 3), seed=41),
+                                           g.protein_chains(100, 500, 0.01, seed=42),
+                                           g.uniform_random(50000, 100.0 * 5 ** (1 / 3), 0.5, 2.0, 43))]
+    x = np.concatenate([p[0] for p in pairs])
+    y = np.concatenate([p[1] for p in pairs])
+    ck = np.concatenate([p[2] for p in pairs])
+    m = P.Model.initial(x, seed=7)
+    m.train(x, y, epochs=4)
+    m.margin = P.choose_margin(m, x, ck)
+    return m
+
+
 def _build(apo, sites, model):
     from apo_b200 import proposal as P
     algo = apo.AlgorithmGPU(sites)
@@ -119,12 +139,11 @@ def _build(apo, sites, model):
 
 
 @pytest.mark.parametrize("kind", ["lognormal", "protein"])
-def test_learned_form_builds_the_plain_diagram_with_fewer_insertions(P, kind):
+def test_learned_form_builds_the_plain_diagram_with_fewer_insertions(P, model, kind):
     import apo_b200
     from apo_b200 import generators as g
     sites = (g.lognormal_cloud(60000, 400.0 * (60000 / 5e6) ** (1 / 3), seed=31) if kind == "lognormal"
              else g.protein_chains(120, 500, 0.01, seed=32))
-    model = P.Model.load()
     plain = _build(apo_b200, sites, None)
     learned = _build(apo_b200, sites, model)
     for name in ("status", "knn", "known_radii", "vertex_nb", "edge_nb", "vertices", "edges"):
