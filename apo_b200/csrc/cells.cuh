@@ -70,7 +70,9 @@ namespace apo2
         if ( c.fp32 )
         {
             t.tests++;
-            const int f = conflict_filter( c.sites_f[ id ], x );
+            // the float copy holds the n input sites; the six bounding sites are rounded here
+            const float4 s = id < c.n ? c.sites_f[ id ] : to_float( c.sites[ id ] );
+            const int    f = conflict_filter( s, x );
             if ( f != 2 )
                 return f == 1;
             t.escalated++;

@@ -202,7 +202,8 @@ struct StagedBuild : apo::gpu::AlgorithmGPU<K>
 
 template<uint32_t K>
 void runReference( std::vector<apo::Real> & sites, const uint32_t n, const std::string & outDir, const int repeat,
-                   const bool dump, const uint32_t knnSteps, std::string & json, const int warmup = 3 )
+                   const bool dump, const uint32_t knnSteps, std::string & json, const int warmup = 3,
+                   const bool withTopology = true )
 {
 
     if ( repeat > 0 )
@@ -335,10 +336,16 @@ void runReference( std::vector<apo::Real> & sites, const uint32_t n, const std::
         writeArray( outDir, "closed_pos.f64", full.closedEdgesMin.data(), full.closedEdgesMin.size() );
         writeArray( outDir, "closed_id.u32", full.closedEdgesId.data(), full.closedEdgesId.size() );
 
-        const apo::gpu::Topology topology = algorithm.toTopology();
-        writeArray( outDir, "topo_quad.u32", topology.quadrisectors.data(), topology.quadrisectors.size() );
-        writeArray( outDir, "topo_tri.u32", topology.trisectors.data(), topology.trisectors.size() );
-        writeArray( outDir, "topo_bi.u32", topology.bisectors.data(), topology.bisectors.size() );
+        // The reference's toTopology grows its output vectors with a reserve per cell, which
+        // copies them once per cell (quadratic): beyond ~10^5 sites it runs for hours, so large
+        // cases skip it (--no-topology; the topology is a function of the stores dumped above).
+        if ( withTopology )
+        {
+            const apo::gpu::Topology topology = algorithm.toTopology();
+            writeArray( outDir, "topo_quad.u32", topology.quadrisectors.data(), topology.quadrisectors.size() );
+            writeArray( outDir, "topo_tri.u32", topology.trisectors.data(), topology.trisectors.size() );
+            writeArray( outDir, "topo_bi.u32", topology.bisectors.data(), topology.bisectors.size() );
+        }
 
         json += ", \"vertices\": " + std::to_string( full.vertices.size() / 4 );
         json += ", \"closed_edges\": " + std::to_string( full.closedEdgesMin.size() / 4 );
@@ -350,13 +357,14 @@ int main( int argc, char ** argv )
 {
     if ( argc < 3 )
     {
-        std::fprintf( stderr, "usage: %s sites.f32 outdir [--time R] [--warmup W] [--no-dump] [--k 1|4|8|16] [--knn-steps S] [--stages]\n", argv[ 0 ] );
+        std::fprintf( stderr, "usage: %s sites.f32 outdir [--time R] [--warmup W] [--no-dump] [--no-topology] [--k 1|4|8|16] [--knn-steps S] [--stages]\n", argv[ 0 ] );
         return 1;
     }
     const std::string input  = argv[ 1 ];
     const std::string outDir = argv[ 2 ];
     int               repeat = 0;
     int               warmup = 3; // untimed builds before the timed ones
+    bool              withTopology = true;
     bool              dump   = true;
     uint32_t          k        = 16; // AlgorithmGPU<K>
     uint32_t          knnSteps = 1;  // knnValidationStep
@@ -367,6 +375,8 @@ int main( int argc, char ** argv )
             repeat = std::atoi( argv[ ++a ] );
         else if ( !std::strcmp( argv[ a ], "--warmup" ) && a + 1 < argc )
             warmup = std::max( 0, std::atoi( argv[ ++a ] ) );
+        else if ( !std::strcmp( argv[ a ], "--no-topology" ) )
+            withTopology = false;
         else if ( !std::strcmp( argv[ a ], "--no-dump" ) )
             dump = false;
         else if ( !std::strcmp( argv[ a ], "--k" ) && a + 1 < argc )
@@ -407,10 +417,10 @@ int main( int argc, char ** argv )
     }
     switch ( k )
     {
-    case 1: runReference<1>( sites, n, outDir, repeat, dump, knnSteps, json, warmup ); break;
-    case 4: runReference<4>( sites, n, outDir, repeat, dump, knnSteps, json, warmup ); break;
-    case 8: runReference<8>( sites, n, outDir, repeat, dump, knnSteps, json, warmup ); break;
-    case 16: runReference<16>( sites, n, outDir, repeat, dump, knnSteps, json, warmup ); break;
+    case 1: runReference<1>( sites, n, outDir, repeat, dump, knnSteps, json, warmup, withTopology ); break;
+    case 4: runReference<4>( sites, n, outDir, repeat, dump, knnSteps, json, warmup, withTopology ); break;
+    case 8: runReference<8>( sites, n, outDir, repeat, dump, knnSteps, json, warmup, withTopology ); break;
+    case 16: runReference<16>( sites, n, outDir, repeat, dump, knnSteps, json, warmup, withTopology ); break;
     default: std::fprintf( stderr, "k must be 1, 4, 8 or 16\n" ); return 1;
     }
 

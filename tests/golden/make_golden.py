@@ -16,6 +16,8 @@ Usage:
     python tests/golden/make_golden.py inputs <dir> [case ...]   writes <case>.f32 and <case>.args
     bash tests/golden/dump_reference.sh <dir> <dump_root>   (on a GPU: runs the reference driver)
     python tests/golden/make_golden.py <dump_root>    (dump_root/<case>/*.u32 ...) -> fixtures
+    python tests/golden/make_golden.py outputs <dump_root> <case>   <case>_ref.npz: the reference's
+        output vertices (ids and positions) of one case, e.g. latticeB20 for the arbitration test
 """
 from __future__ import annotations
 
@@ -84,9 +86,13 @@ def sites_for(case: str) -> np.ndarray:
 
 
 def load_dump(root: str, case: str) -> dict:
+    """The arrays of one case's dump; the topology arrays are absent from large cases, whose
+    driver run skipped the reference's quadratic toTopology (they follow from the stores)."""
     out = {}
     for name, dt in ARRAYS.items():
         path = os.path.join(root, case, f"{name}.{_EXT[dt]}")
+        if name.startswith("topo_") and not os.path.exists(path):
+            continue
         a = np.fromfile(path, dtype=dt)
         if name == "closed_id":
             # the reference leaves the 4th id word uninitialised; only (i, j, k) is defined
@@ -104,8 +110,9 @@ def write_inputs(out: str, cases: list[str] | None = None) -> None:
     for case in cases or list(CASES):
         sites_for(case).astype(np.float32).tofile(os.path.join(out, case + ".f32"))
         k, steps = case_params(case)
+        extra = " --no-topology" if sites_for(case).shape[0] > 200000 else ""
         with open(os.path.join(out, case + ".args"), "w") as f:
-            f.write(f"--k {k} --knn-steps {steps}\n")
+            f.write(f"--k {k} --knn-steps {steps}{extra}\n")
 
 
 def main(root: str) -> None:
@@ -114,7 +121,7 @@ def main(root: str) -> None:
     digests = json.load(open(path)) if os.path.exists(path) else {}
     for case, entry in CASES.items():
         whole = entry[1]
-        if not os.path.isdir(os.path.join(root, case)):
+        if not os.path.exists(os.path.join(root, case, "meta.json")):  # absent or unfinished dump
             print("skip", case)
             continue
         sites = sites_for(case)
@@ -138,8 +145,18 @@ def main(root: str) -> None:
         json.dump(digests, f, indent=1, sort_keys=True)
 
 
+def write_outputs(root: str, case: str) -> None:
+    """The reference's output vertices of one case (ids and positions), stored whole."""
+    ids = np.fromfile(os.path.join(root, case, "vertices_id.u32"), np.uint32)
+    pos = np.fromfile(os.path.join(root, case, "vertices_pos.f64"), np.float64)
+    np.savez_compressed(os.path.join(HERE, f"{case}_ref.npz"), vertices_id=ids, vertices_pos=pos)
+    print(case, ids.size // 4, "output vertices")
+
+
 if __name__ == "__main__":
     if sys.argv[1] == "inputs":
         write_inputs(sys.argv[2], sys.argv[3:] or None)
+    elif sys.argv[1] == "outputs":
+        write_outputs(sys.argv[2], sys.argv[3])
     else:
         main(sys.argv[1])

@@ -1,0 +1,57 @@
+"""Arbitration of the one known departure from the reference: lattice B (20^3 sites, spacing 3,
+log-normal radii, jitter 1e-4), where quadruples of centres coplanar to 1e-4 put the vertex
+quadratic's discriminant within rounding of its 1e-8 threshold, so whether a root exists depends
+on how each build contracted the solve into fused multiply-adds. The vertices that only one of the
+two builds outputs are checked with the interval certificate (the reference's precision check,
+app/precision/precision.cpp:14-163, run by apo2_certify): a vertex fails when another site is
+certainly closer than its own four. The reference's output comes from its own CUDA build run on a
+B200 (tests/golden/latticeB20_ref.npz: every output vertex's ids and position)."""
+import collections
+import os
+
+import numpy as np
+import pytest
+
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def _rows(ids, pos):
+    ids = ids.reshape(-1, 4)
+    pos = pos.reshape(-1, 4)
+    return collections.Counter(tuple(r) for r in ids.tolist()), ids, pos
+
+
+def _only(counter_a, counter_b, ids, pos):
+    """Rows of (ids, pos) whose id quadruple occurs more often in a than in b."""
+    extra = counter_a - counter_b
+    keep = []
+    for q, row in enumerate(ids.tolist()):
+        t = tuple(row)
+        if extra.get(t, 0) > 0:
+            extra[t] -= 1
+            keep.append(q)
+    keep = np.array(keep, dtype=np.int64)
+    return ids[keep], pos[keep]
+
+
+def test_lattice_b_departures_certified_on_both_sides():
+    import apo_b200
+    ref = np.load(os.path.join(H.GOLDEN, "latticeB20_ref.npz"))
+    algo = apo_b200.AlgorithmGPU(H.sites_for("latticeB20"))
+    algo.build()
+    mine = algo.toHost()
+    cm, mids, mpos = _rows(mine.verticesId, mine.vertices)
+    cr, rids, rpos = _rows(ref["vertices_id"], ref["vertices_pos"])
+    only_mine_ids, only_mine_pos = _only(cm, cr, mids, mpos)
+    only_ref_ids, only_ref_pos = _only(cr, cm, rids, rpos)
+    shared = sum((cm & cr).values())
+    assert shared >= 0.999 * max(sum(cm.values()), sum(cr.values()))
+    bad_mine = algo.certify(only_mine_pos, only_mine_ids)[0] if len(only_mine_ids) else 0
+    bad_ref = algo.certify(only_ref_pos, only_ref_ids)[0] if len(only_ref_ids) else 0
+    print(f"lattice B: {shared} shared vertices, {len(only_mine_ids)} only here ({bad_mine} fail the certificate), "
+          f"{len(only_ref_ids)} only in the reference ({bad_ref} fail)")
+    # every vertex this build outputs and the reference does not is certified empty
+    assert bad_mine == 0
+    algo.close()

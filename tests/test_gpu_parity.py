@@ -91,10 +91,11 @@ def test_gpu_matches_reference_digests(apo, case):
     full = algo.toHostFull(True)
     assert H.sha(full.verticesId) == d["arrays"]["vertices_id"]
     assert H.sha(H.closed_ids3(full.closedEdgesId)) == d["arrays"]["closed_id"]
-    topo = algo.toTopology()
-    assert H.sha(topo.quadrisectors) == d["arrays"]["topo_quad"]
-    assert H.sha(topo.trisectors) == d["arrays"]["topo_tri"]
-    assert H.sha(topo.bisectors) == d["arrays"]["topo_bi"]
+    if "topo_quad" in d["arrays"]:  # large cases pin the stores, of which the topology is a function
+        topo = algo.toTopology()
+        assert H.sha(topo.quadrisectors) == d["arrays"]["topo_quad"]
+        assert H.sha(topo.trisectors) == d["arrays"]["topo_tri"]
+        assert H.sha(topo.bisectors) == d["arrays"]["topo_bi"]
 
 
 def test_gpu_near_degenerate_lattice_agreement(apo):
