@@ -63,7 +63,8 @@ class Stats(ctypes.Structure):
                 ("ms_output", ctypes.c_double), ("device_bytes", ctypes.c_uint64), ("uncertified", ctypes.c_uint32),
                 ("reserved32", ctypes.c_uint32), ("knn_insertions", ctypes.c_uint64), ("proposal_cells", ctypes.c_uint64),
                 ("proposal_fallbacks", ctypes.c_uint64), ("proposal_skipped", ctypes.c_uint64),
-                ("filter_tests", ctypes.c_uint64), ("filter_escalations", ctypes.c_uint64)]
+                ("filter_tests", ctypes.c_uint64), ("filter_escalations", ctypes.c_uint64),
+                ("proposal_second_step", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("reserved")}
@@ -359,7 +360,7 @@ class AlgorithmGPU:
     _DEBUG_DTYPES = {"indices": np.uint32, "parent": np.int32, "left": np.int32, "right": np.int32,
                      "aabb": np.float32, "sizes": np.uint32, "morton": np.uint64, "sites_sorted": np.float64,
                      "status": np.uint8, "knn": np.uint32, "known_radii": np.float32, "vertex_nb": np.uint32,
-                     "edge_nb": np.uint32, "vertices": np.uint32, "edges": np.uint32}
+                     "edge_nb": np.uint32, "vertices": np.uint32, "edges": np.uint32, "proposed_k": np.uint8}
 
     def debug_array(self, name: str) -> np.ndarray:
         """Internal array by name (sorted-space ids), for parity checks."""

@@ -241,6 +241,12 @@ namespace
                 record( h, 3, s );
             launch_cells( h->cells, step == 0 ? kCellsFirst : kCellsNext, s );
         }
+        if ( h->cells.scheduled )
+        {
+            // learned form: a second kNN step for the uncertified cells proposed beyond k
+            launch_knn( h->cells, 1, s );
+            launch_cells( h->cells, kCellsNext, s );
+        }
         record( h, 4, s );
         // stop_after (parity checks): 1 after the cells, 2 + 2r / 3 + 2r after round r's passes
         const uint32_t stop   = h->options.stop_after;
@@ -1112,10 +1118,15 @@ apo2_status apo2_contribution_profile( apo2_handle * h, uint32_t steps, uint8_t 
         launch_bounds( h->input, h->input_f64, n, h->input_d4, h->partials, h->partial_count, h->bounds_counter, h->scene,
                        h->tree.sites + n, s );
         launch_tree( h->tree, n, h->input_d4, h->scene, h->sort, s, h->options.wait_limit );
+        // the labels are the plain construction's: no proposal takes part
+        CellContext plain  = h->cells;
+        plain.proposal     = nullptr;
+        plain.proposed_k   = nullptr;
+        plain.scheduled    = 0;
         for ( uint32_t step = 0; step < steps; step++ )
         {
-            launch_knn( h->cells, step, s );
-            launch_cells_profile( h->cells, step, row, dc, dr, s );
+            launch_knn( plain, step, s );
+            launch_cells_profile( plain, step, row, dc, dr, s );
         }
     }
     uint32_t    err = 0;
@@ -1213,6 +1224,12 @@ apo2_status apo2_debug_array( apo2_handle * h, const char * name, void * dst, ui
         src = h->cells.knn, elems = uint64_t( n ) * h->cells.k;
     else if ( key == "known_radii" )
         src = h->cells.known_radii, elems = n;
+    else if ( key == "proposed_k" )
+    {
+        if ( !h->cells.proposed_k )
+            return fail( APO2_ERR_INVALID_ARG, "no k-proposal attached" );
+        src = h->cells.proposed_k, elems = n, esize = 1;
+    }
     else if ( key == "vertex_nb" )
         src = h->cells.vertex_nb, elems = n;
     else if ( key == "edge_nb" )
@@ -1284,6 +1301,7 @@ apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
     s.proposal_fallbacks = cnt[ kCountFallbacks ];
     s.proposal_skipped   = cnt[ kCountSkipped ];
     s.filter_tests       = cnt[ kCountFiltered ];
+    s.proposal_second_step = cnt[ kCountSecondStep ];
     s.filter_escalations = cnt[ kCountEscalated ];
     s.kernel_launches = h->launches;
     if ( h->timing )
@@ -1349,18 +1367,27 @@ apo2_status apo2_set_proposal( apo2_handle * h, const apo2_proposal * model )
     APO2_CUDA( cudaDeviceSynchronize(), "set proposal" ); // no build may still read the old model
     if ( !model )
     {
-        h->cells.proposal   = nullptr;
-        h->cells.proposed_k = nullptr;
+        h->cells.proposal     = nullptr;
+        h->cells.proposed_k   = nullptr;
+        h->cells.scheduled    = 0;
+        h->cells.proposal_max = 0;
         return APO2_OK;
     }
+    const uint32_t k = h->cells.k;
+    if ( model->max_rank > std::min( 2 * k, 255u ) )
+        return fail( APO2_ERR_INVALID_ARG, "apo2_proposal.max_rank is at most 2K" );
     if ( !h->proposal_alloc )
         APO2_CUDA( cudaMalloc( &h->proposal_alloc, align256( sizeof( ProposalNet ) ) + align256( h->n ) ), "proposal allocation" );
     char * p = static_cast<char *>( h->proposal_alloc );
-    APO2_CUDA( cudaMemcpy( p, reinterpret_cast<const char *>( model ) + 2 * sizeof( uint32_t ), sizeof( ProposalNet ),
+    APO2_CUDA( cudaMemcpy( p, reinterpret_cast<const char *>( model ) + kProposalHeader, sizeof( ProposalNet ),
                            cudaMemcpyHostToDevice ),
                "proposal upload" );
-    h->cells.proposal   = reinterpret_cast<const ProposalNet *>( p );
-    h->cells.proposed_k = reinterpret_cast<uint8_t *>( p + align256( sizeof( ProposalNet ) ) );
+    h->cells.proposal     = reinterpret_cast<const ProposalNet *>( p );
+    h->cells.proposed_k   = reinterpret_cast<uint8_t *>( p + align256( sizeof( ProposalNet ) ) );
+    h->cells.proposal_max = model->max_rank ? model->max_rank : k;
+    // the second step applies to builds of one configured kNN step; with several, every cell
+    // takes them all (the reference's schedule) and proposals only place the first check
+    h->cells.scheduled = ( h->cells.proposal_max > k && h->options.knn_steps == 1 ) ? 1u : 0u;
     return APO2_OK;
 }
 

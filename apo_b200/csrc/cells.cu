@@ -718,6 +718,9 @@ namespace apo2
         const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
         if ( id >= c.n )
             return;
+        // learned form's second step: only the uncertified cells proposed beyond k search again
+        if ( step != 0 && c.scheduled && ( !second_step_cell( c, id ) || c.status[ id ] != kInValidation ) )
+            return;
         const uint32_t k      = c.k;
         const uint32_t n      = c.n;
         const float4   si     = c.sites_f[ id ];
@@ -834,7 +837,7 @@ namespace apo2
             in.n       = n;
             float f[ kPIn ];
             proposal_features( in, id, keys, stride, k, f );
-            c.proposed_k[ id ] = uint8_t( proposal_rank( s_net[ 0 ], proposal_predict( s_net[ 0 ], f ), k ) );
+            c.proposed_k[ id ] = uint8_t( proposal_rank( s_net[ 0 ], proposal_predict( s_net[ 0 ], f ), c.proposal_max ) );
         }
 
         // buried site: inside its nearest neighbour (algorithm.inl:85-98); `si` is the float copy
@@ -920,9 +923,15 @@ namespace apo2
             const uint8_t status = c.status[ i ];
             if ( status == kFullyValidated || ( mode == kCellsNext && status == kBuried ) )
                 continue;
+            if ( mode == kCellsNext && c.scheduled && !second_step_cell( c, i ) )
+                continue; // learned form: this cell was proposed within k, so it has one step only
             const double4 si = c.sites[ i ];
             if ( mode == kCellsNext )
+            {
                 load_cell( c, w, i, si, true, true );
+                if ( c.scheduled && lane_id() == 0 )
+                    counts[ kCountSecondStep ]++;
+            }
             else
                 initial_cell( c, w, si );
             if ( status == kBuried )
@@ -935,7 +944,15 @@ namespace apo2
             // learned form: the certificate is first checked at the proposed rank; a cell that
             // passes there stops inserting (its later neighbours cannot change a certified cell)
             // but its known radius still covers its whole list, as the plain form's does
-            const uint32_t check_at = ( c.proposed_k && mode == kCellsFirst ) ? c.proposed_k[ i ] : c.k;
+            uint32_t check_at = c.k;
+            if ( c.proposed_k )
+            {
+                const uint32_t r = c.proposed_k[ i ];
+                if ( mode == kCellsFirst )
+                    check_at = min( r, c.k );
+                else if ( c.scheduled )
+                    check_at = r > c.k ? r - c.k : c.k; // rank r counts the first step's k neighbours
+            }
             double         known    = -DBL_MAX;
             bool           done     = false;
             for ( uint32_t q = 0; q < c.k; q++ )

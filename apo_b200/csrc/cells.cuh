@@ -48,6 +48,8 @@ namespace apo2
         const ProposalNet * proposal   = nullptr;
         const uint64_t *    codes      = nullptr;
         uint8_t *           proposed_k = nullptr;
+        uint32_t            proposal_max = 0; // largest proposed rank (k .. 2k)
+        uint32_t            scheduled    = 0; // 1: cells proposed beyond k get a second kNN step
         // build counters: kNN insertions, cells checked at a proposed rank, fallbacks, skipped
         // neighbours, conflict predicates decided by the FP32 filter, those it left to FP64
         unsigned long long * counters = nullptr;
@@ -55,7 +57,13 @@ namespace apo2
         uint32_t fp32 = 0;
     };
     constexpr uint32_t kCountInsertions = 0, kCountChecked = 1, kCountFallbacks = 2, kCountSkipped = 3, kCountFiltered = 4,
-                       kCountEscalated = 5, kCounters = 6;
+                       kCountEscalated = 5, kCountSecondStep = 6, kCounters = 7;
+
+    // Learned form with a second kNN step: is cell i one of those proposed beyond k?
+    __device__ __forceinline__ bool second_step_cell( const CellContext & c, uint32_t i )
+    {
+        return c.scheduled && c.proposed_k[ i ] > c.k;
+    }
 
     // Lane-local tallies of the FP32 filter, added to the build's counters when a kernel ends.
     struct FilterTally

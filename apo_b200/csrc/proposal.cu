@@ -346,7 +346,7 @@ extern "C" apo2_status apo2_proposal_predict( const apo2_proposal * model, const
     ProposalNet * net = reinterpret_cast<ProposalNet *>( p );
     float *       x   = reinterpret_cast<float *>( p + ( ( sizeof( ProposalNet ) + 255 ) & ~size_t( 255 ) ) );
     float *       o   = x + n * kPIn;
-    cudaError_t   e   = cudaMemcpy( net, reinterpret_cast<const char *>( model ) + 2 * sizeof( uint32_t ), sizeof( ProposalNet ),
+    cudaError_t   e   = cudaMemcpy( net, reinterpret_cast<const char *>( model ) + kProposalHeader, sizeof( ProposalNet ),
                                     cudaMemcpyHostToDevice );
     if ( e == cudaSuccess )
         e = cudaMemcpy( x, features, sizeof( float ) * n * kPIn, cudaMemcpyHostToDevice );

@@ -36,7 +36,9 @@ namespace apo2
         __nv_bfloat16 w2[ kPHid * kPHid ];
         __nv_bfloat16 w3[ kPHid ];
     };
-    static_assert( sizeof( ProposalNet ) == sizeof( apo2_proposal ) - 2 * sizeof( uint32_t ), "layout of apo2_proposal" );
+    // ProposalNet is apo2_proposal without its three leading words
+    constexpr size_t kProposalHeader = 3 * sizeof( uint32_t );
+    static_assert( sizeof( ProposalNet ) == sizeof( apo2_proposal ) - kProposalHeader, "layout of apo2_proposal" );
 
     // Feature vector of site i (sorted order) from its sorted kNN list; see proposal.cu.
     struct FeatureInputs
@@ -49,11 +51,11 @@ namespace apo2
 
     void launch_features( const FeatureInputs & in, const uint32_t * knn, uint32_t k, float * out, cudaStream_t s );
 
-    // Predicted log2 rank; the proposed rank is ceil(2^(prediction + margin)) clamped to [1, k].
-    __device__ __forceinline__ uint32_t proposal_rank( const ProposalNet & net, float prediction, uint32_t k )
+    // Predicted log2 rank; the proposed rank is ceil(2^(prediction + margin)) clamped to [1, max_rank].
+    __device__ __forceinline__ uint32_t proposal_rank( const ProposalNet & net, float prediction, uint32_t max_rank )
     {
         const float r = ceilf( exp2f( fminf( prediction + net.margin, 30.f ) ) );
-        return r < 1.f ? 1u : ( r >= float( k ) ? k : uint32_t( r ) );
+        return r < 1.f ? 1u : ( r >= float( max_rank ) ? max_rank : uint32_t( r ) );
     }
     // -----------------------------------------------------------------------------------
     // Features and inference

@@ -1,7 +1,7 @@
 """Trains the learned k-proposal shipped as apo_b200/models/proposal_k16.npz (needs a GPU).
 
-Training data: (features, certified rank) pairs logged by the plain construction (K = 16, one kNN
-step) on 200 diagrams of about 100,000 sites each, drawn with random seeds from the generators of
+Training data: (features, certified rank) pairs logged by the plain construction (K = 16, two kNN
+steps: ranks 1..32) on 200 diagrams of about 100,000 sites each, drawn with random seeds from the generators of
 the plain workloads: uniform clouds (the reference's getUniform formula at its 10,000-site density),
 protein-like packings (self-avoiding chains) and the near-degenerate lattices A and B. Every
 feature, label and gradient is computed by the library's own kernels; the margin is then chosen
@@ -71,10 +71,14 @@ def main():
     model.save(args.out)
     r = model.ranks(X[held])
     ok = (R[held] > 0) & (R[held] <= r)
+    plain = P.expected_cost(np.full(held.sum(), P.K), R[held]).mean()
+    learned = P.expected_cost(r, R[held]).mean()
     summary = {
         "pairs": int(X.shape[0]), "held_out": int(held.sum()), "epochs": args.epochs, "loss": losses.tolist(),
         "margin": model.margin, "data_seconds": round(t_data, 1), "train_seconds": round(t_train, 2),
         "held_out_certified_at_proposal": float(ok.mean()),
+        "held_out_second_step_share": float((r > P.K).mean()),
+        "held_out_expected_cost": {"plain": plain, "learned": learned},
         "held_out_mean_proposal": float(r.mean()),
         "held_out_mean_certified_rank": float(R[held][R[held] > 0].mean()),
         "label_share_not_certified": float((R == 0).mean()),

@@ -8,8 +8,8 @@ ABI in include/apo2.h); this module prepares data and drives the calls.
 
 Labels are the reference's own measurement (app/benchmarks/benchmark_contributing_nearest.cu:
 10-129, restated as apo2_contribution_profile): the rank at which the certificate first held
-during the plain construction. A cell that does not certify within the list gets the label
-log2(K) + 1 (its proposal is then the whole list, which is the plain form).
+during the plain construction with two kNN steps (ranks 1..2K). A cell that does not certify
+within them gets the label log2(2K) + 1.
 """
 from __future__ import annotations
 
@@ -21,13 +21,14 @@ import numpy as np
 from . import APO2_ERR_ITER_LIMIT, AlgorithmGPU, Apo2Error, _check, load_library
 
 INPUTS, HIDDEN = 16, 64
+K = 16  # the reference's kNN list length, which the shipped model is trained for
 PARAMS = HIDDEN * INPUTS + HIDDEN + HIDDEN * HIDDEN + HIDDEN + HIDDEN + 1  # 5,313
 DEFAULT_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "proposal_k16.npz")
 
 
 class Proposal(ctypes.Structure):
     """apo2_proposal (include/apo2.h)."""
-    _fields_ = [("struct_size", ctypes.c_uint32), ("version", ctypes.c_uint32),
+    _fields_ = [("struct_size", ctypes.c_uint32), ("version", ctypes.c_uint32), ("max_rank", ctypes.c_uint32),
                 ("mean", ctypes.c_float * INPUTS), ("inv_scale", ctypes.c_float * INPUTS),
                 ("margin", ctypes.c_float), ("b3", ctypes.c_float),
                 ("b1", ctypes.c_float * HIDDEN), ("b2", ctypes.c_float * HIDDEN),
@@ -42,12 +43,14 @@ def _sig():
 class Model:
     """A trained (or initial) network: the fp32 parameter vector and the bf16 model the GPU reads."""
 
-    def __init__(self, master: np.ndarray, mean: np.ndarray, inv_scale: np.ndarray, margin: float = 0.0):
+    def __init__(self, master: np.ndarray, mean: np.ndarray, inv_scale: np.ndarray, margin: float = 0.0,
+                 max_rank: int = 2 * K):
         self.master = np.ascontiguousarray(master, dtype=np.float32)
         assert self.master.size == PARAMS
         self.mean = np.ascontiguousarray(mean, dtype=np.float32)
         self.inv_scale = np.ascontiguousarray(inv_scale, dtype=np.float32)
         self.margin = float(margin)
+        self.max_rank = int(max_rank)
 
     @staticmethod
     def initial(features: np.ndarray, seed: int = 0) -> "Model":
@@ -68,6 +71,7 @@ class Model:
         p = Proposal()
         p.struct_size = ctypes.sizeof(Proposal)
         p.version = 1
+        p.max_rank = self.max_rank
         p.mean[:] = self.mean.tolist()
         p.inv_scale[:] = self.inv_scale.tolist()
         p.margin = self.margin
@@ -94,11 +98,11 @@ class Model:
         _check(lib.apo2_proposal_predict(ctypes.byref(p), x.ctypes.data, x.shape[0], out.ctypes.data))
         return out
 
-    def ranks(self, features: np.ndarray, k: int = 16) -> np.ndarray:
-        """Proposed ranks ceil(2^(prediction + margin)) in [1, k], as the kNN kernel computes them."""
+    def ranks(self, features: np.ndarray) -> np.ndarray:
+        """Proposed ranks ceil(2^(prediction + margin)) in [1, max_rank], as the kNN kernel computes them."""
         pred = self.predict(features).astype(np.float32)
         r = np.ceil(np.exp2(np.minimum(pred + np.float32(self.margin), 30.0)))
-        return np.clip(r, 1, k).astype(np.int64)
+        return np.clip(r, 1, self.max_rank).astype(np.int64)
 
     def gradients(self, features: np.ndarray, targets: np.ndarray) -> tuple[float, np.ndarray]:
         """Loss and gradient of one batch from the GPU training kernels."""
@@ -128,12 +132,14 @@ class Model:
 
     def save(self, path: str) -> None:
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
-        np.savez(path, master=self.master, mean=self.mean, inv_scale=self.inv_scale, margin=np.float32(self.margin))
+        np.savez(path, master=self.master, mean=self.mean, inv_scale=self.inv_scale, margin=np.float32(self.margin),
+                 max_rank=np.int32(self.max_rank))
 
     @staticmethod
     def load(path: str = DEFAULT_MODEL) -> "Model":
         with np.load(path) as z:
-            return Model(z["master"], z["mean"], z["inv_scale"], float(z["margin"]))
+            max_rank = int(z["max_rank"]) if "max_rank" in z.files else K
+            return Model(z["master"], z["mean"], z["inv_scale"], float(z["margin"]), max_rank)
 
 
 def _bf16_bits(a: np.ndarray) -> np.ndarray:
@@ -159,15 +165,15 @@ def features(algo: AlgorithmGPU) -> np.ndarray:
     return out
 
 
-def labels(certified_k: np.ndarray, k: int = 16) -> np.ndarray:
-    """log2 of the certified rank (1..k), log2(k) + 1 for cells that did not certify."""
+def labels(certified_k: np.ndarray, max_rank: int = 2 * K) -> np.ndarray:
+    """log2 of the certified rank (1..max_rank), log2(max_rank) + 1 for cells that did not certify."""
     ck = np.asarray(certified_k)
-    return np.where(ck > 0, np.log2(np.maximum(ck, 1)), np.log2(k) + 1.0).astype(np.float32)
+    return np.where(ck > 0, np.log2(np.maximum(ck, 1)), np.log2(max_rank) + 1.0).astype(np.float32)
 
 
 def training_pairs(sites: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     """(features, targets, certified rank) of every non-buried site of one site set, from the
-    plain construction with K = 16 and one kNN step."""
+    plain construction with K = 16 and two kNN steps (ranks 1..32)."""
     algo = AlgorithmGPU(sites)
     try:
         algo.build()
@@ -178,23 +184,40 @@ def training_pairs(sites: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarra
             raise
     f = features(algo)
     status = algo.debug_array("status")
-    _, _, ck = algo.contribution_profile(steps=1)
+    _, _, ck = algo.contribution_profile(steps=2)
     algo.close()
     keep = status != 0xFF
     return f[keep], labels(ck[keep]), ck[keep]
 
 
-def choose_margin(model: Model, features: np.ndarray, certified_k: np.ndarray, k: int = 16, check_cost: float = 1.0) -> float:
-    """Margin minimising the expected work of a cell on held-out data: neighbours inserted
-    (up to its proposal when it certifies there, all k otherwise) plus `check_cost` insertions
-    per failed early check."""
-    pred = model.predict(features).astype(np.float64)
+def expected_cost(ranks: np.ndarray, certified_k: np.ndarray, k: int = K, validation: float = 120.0,
+                  check: float = 1.0, second_search: float = 2.0) -> np.ndarray:
+    """Work of each cell, in neighbour insertions, when its certificate is checked at `ranks`:
+    insertions up to where it certifies, a failed check, the second kNN search of a cell proposed
+    beyond k, and the validation passes of a cell that does not certify by kNN (`validation`:
+    about 120 insertions of time per cell on the B200, from the stage times of the plain form)."""
+    r = np.asarray(ranks, np.float64)
     ck = np.asarray(certified_k)
+    cert = ck > 0
+    one = r <= k
+    # proposed within k: certifies at r, at the end of the list, or goes to validation
+    c1 = np.where(cert & (ck <= r), r,
+                  np.where(cert & (ck <= k), k + check, k + np.where(r < k, check, 0.0) + validation))
+    # proposed beyond k: the first list, then the second step when still uncertified
+    c2 = np.where(cert & (ck <= k), k,
+                  np.where(cert & (ck <= r), r + second_search,
+                           np.where(cert & (ck <= 2 * k), 2 * k + second_search + check,
+                                    2 * k + second_search + np.where(r < 2 * k, check, 0.0) + validation)))
+    return np.where(one, c1, c2)
+
+
+def choose_margin(model: Model, features: np.ndarray, certified_k: np.ndarray, k: int = K) -> float:
+    """Margin minimising the expected work per cell (expected_cost) on held-out data."""
+    pred = model.predict(features).astype(np.float64)
     best, best_cost = 0.0, np.inf
-    for m in np.arange(-1.0, 2.01, 0.125):
-        r = np.clip(np.ceil(np.exp2(pred + m)), 1, k)
-        ok = (ck > 0) & (ck <= r)
-        cost = np.where(ok, r, k + np.where(r < k, check_cost, 0.0)).mean()
+    for m in np.arange(-2.0, 2.01, 0.125):
+        r = np.clip(np.ceil(np.exp2(pred + m)), 1, model.max_rank)
+        cost = expected_cost(r, certified_k, k).mean()
         if cost < best_cost:
             best, best_cost = float(m), float(cost)
     return best

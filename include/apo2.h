@@ -133,6 +133,7 @@ typedef struct apo2_stats
     uint64_t proposal_skipped;     /* neighbours not inserted because the cell certified earlier */
     uint64_t filter_tests;         /* FP32-filtered form: conflict predicates of the cell kernels */
     uint64_t filter_escalations;   /* ... that fell inside the bound and were evaluated in FP64 */
+    uint64_t proposal_second_step; /* learned form: cells that took the second kNN step */
 } apo2_stats;
 
 /* Library version string. */
@@ -215,11 +216,17 @@ apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint3
  * ReLU, bf16 weights and fp32 accumulation predicts log2 of the kNN rank at which a site's cell
  * passes the security-radius certificate, from 16 features of the site (radius, Morton-local
  * density, radii and distances of its nearest neighbours; see apo2_proposal_features). With a
- * model attached (apo2_set_proposal), the kNN kernel runs the network for every site and the kNN
- * cell construction checks the certificate at the proposed rank ceil(2^(prediction + margin)):
- * a cell that passes stops there (the later neighbours of its list cannot change a certified
- * cell), one that does not goes on through the rest of its list as the plain method does (a
- * fallback). Either way the certificate alone decides. */
+ * model attached (apo2_set_proposal), the kNN kernel runs the network for every site and each cell
+ * gets the proposed rank ceil(2^(prediction + margin)) in [1, max_rank]:
+ *   - a rank r <= K: the kNN cell construction checks the certificate after r neighbours; a cell
+ *     that passes stops there (its later neighbours cannot change a certified cell), one that
+ *     does not (a fallback) goes on through its list as the plain form does;
+ *   - a rank r > K (max_rank > K, with one kNN step configured): the cell goes through its K
+ *     neighbours, then -- if still uncertified -- through a second kNN step, the next K sites
+ *     beyond the last (the reference's expanding search, knnValidationStep = 2,
+ *     algorithm.inl:1535-1549), with its certificate checked after r - K of them.
+ * Either way the certificate alone decides, and every cell ends as the reference's build with one
+ * kNN step (r <= K) or two (r > K) leaves it. */
 #define APO2_PROPOSAL_INPUTS 16
 #define APO2_PROPOSAL_HIDDEN 64
 #define APO2_PROPOSAL_PARAMS 5313 /* fp32 training vector: W1 (64 x 16), b1, W2 (64 x 64), b2, w3, b3 */
@@ -228,6 +235,9 @@ typedef struct apo2_proposal
 {
     uint32_t struct_size;                                         /* sizeof(apo2_proposal) */
     uint32_t version;                                             /* 1 */
+    uint32_t max_rank;                                            /* largest proposed rank: K (early checks
+                                                                     only) up to 2K (a second kNN step for
+                                                                     cells proposed beyond K) */
     float    mean[ APO2_PROPOSAL_INPUTS ];                        /* inputs are (x - mean) * inv_scale */
     float    inv_scale[ APO2_PROPOSAL_INPUTS ];
     float    margin;                                              /* added to the prediction before 2^() */
@@ -330,7 +340,7 @@ apo2_status apo2_get_cell( apo2_handle * h, uint32_t site, uint32_t * vertices, 
  * (sorted -> original id, u32[n]), "parent", "left", "right" (i32[2n-1]), "aabb"
  * (f32[8(2n-1)], min xyz 0 max xyz 0), "sizes" (u32[2n-1]), "morton" (u64[n], sorted),
  * "sites_sorted" (f64[4(n+6)]), "status" (u8[n]), "knn" (u32[n*k]), "known_radii"
- * (f32[n]), "vertex_nb", "edge_nb" (u32[n]), "vertices", "edges" (u32 records of 4 words,
+ * (f32[n]), "proposed_k" (u8[n], the learned form's proposed ranks), "vertex_nb", "edge_nb" (u32[n]), "vertices", "edges" (u32 records of 4 words,
  * cells in sorted order, sorted-space ids). With dst == NULL only *count is set (elements). */
 apo2_status apo2_debug_array( apo2_handle * h, const char * name, void * dst, uint64_t capacity_bytes,
                               uint64_t * count );

@@ -138,30 +138,75 @@ def _build(apo, sites, model):
     return algo
 
 
+def _per_cell(algo, name, counts):
+    """Per-cell store records (4 words each) as a list of arrays, cells in sorted order."""
+    flat = algo.debug_array(name).reshape(-1, 4)
+    ends = np.cumsum(counts.astype(np.int64))
+    return np.split(flat, ends[:-1])
+
+
 @pytest.mark.parametrize("kind", ["lognormal", "protein"])
-def test_learned_form_builds_the_plain_diagram_with_fewer_insertions(P, model, kind):
+def test_learned_form_builds_the_reference_cells(P, model, kind):
+    """Every cell of the learned form ends as the reference's build leaves it with one kNN step
+    (proposed rank <= 16) or two (proposed beyond 16): status, known radius, both stores record by
+    record, and the output vertices the cell owns."""
     import apo_b200
     from apo_b200 import generators as g
     sites = (g.lognormal_cloud(60000, 400.0 * (60000 / 5e6) ** (1 / 3), seed=31) if kind == "lognormal"
              else g.protein_chains(120, 500, 0.01, seed=32))
-    plain = _build(apo_b200, sites, None)
+    one = apo_b200.AlgorithmGPU(sites, knnValidationStep=1)
+    one.build()
+    two = apo_b200.AlgorithmGPU(sites, knnValidationStep=2)
+    two.build()
     learned = _build(apo_b200, sites, model)
-    for name in ("status", "knn", "known_radii", "vertex_nb", "edge_nb", "vertices", "edges"):
-        assert np.array_equal(learned.debug_array(name), plain.debug_array(name)), name
-    a, b = learned.toHostFull(True), plain.toHostFull(True)
-    assert np.array_equal(a.verticesId, b.verticesId)
-    assert np.array_equal(a.vertices, b.vertices)
-    assert np.array_equal(a.closedEdgesId, b.closedEdgesId)
-    sp, sl = plain.stats(), learned.stats()
-    assert sp["proposal_cells"] == 0 and sl["proposal_cells"] > 0
-    assert sl["proposal_skipped"] > 0
-    # what the trained network gains over the method without it
-    assert sl["knn_insertions"] + sl["proposal_skipped"] == sp["knn_insertions"]
-    assert sl["knn_insertions"] < sp["knn_insertions"]
-    # ... and over an untrained network (He-initialised, no margin search)
-    untrained = P.Model.initial(P.features(plain), seed=99)
-    rough = _build(apo_b200, sites, untrained)
-    assert np.array_equal(rough.debug_array("vertices"), plain.debug_array("vertices"))
-    assert sl["knn_insertions"] + sl["proposal_fallbacks"] < rough.stats()["knn_insertions"] + rough.stats()["proposal_fallbacks"]
-    for x in (plain, learned, rough):
+    sel = learned.debug_array("proposed_k") > 16
+    for name in ("status", "known_radii", "vertex_nb", "edge_nb"):
+        want = np.where(sel, two.debug_array(name), one.debug_array(name))
+        assert np.array_equal(learned.debug_array(name), want), name
+    for name, counts in (("vertices", "vertex_nb"), ("edges", "edge_nb")):
+        mine = _per_cell(learned, name, learned.debug_array(counts))
+        a = _per_cell(one, name, one.debug_array(counts))
+        b = _per_cell(two, name, two.debug_array(counts))
+        for i in range(len(mine)):
+            assert np.array_equal(mine[i], b[i] if sel[i] else a[i]), (name, i)
+    inv = np.empty(sites.shape[0], np.int64)
+    inv[learned.debug_array("indices")] = np.arange(sites.shape[0])
+
+    def owned_rows(algo, chosen):
+        v = algo.toHost()
+        ids = v.verticesId.reshape(-1, 4)
+        keep = sel[inv[ids[:, 0]]] == chosen
+        return ids[keep], v.vertices.reshape(-1, 4)[keep]
+    mi, mp = learned.toHost().verticesId.reshape(-1, 4), learned.toHost().vertices.reshape(-1, 4)
+    ai, ap = owned_rows(one, False)
+    bi, bp = owned_rows(two, True)
+    wi, wp = np.concatenate([ai, bi]), np.concatenate([ap, bp])
+    order_m = np.lexsort(np.concatenate([mi, mp.view(np.int64)], axis=1).T[::-1])
+    order_w = np.lexsort(np.concatenate([wi, wp.view(np.int64)], axis=1).T[::-1])
+    assert np.array_equal(mi[order_m], wi[order_w])
+    assert np.array_equal(mp[order_m], wp[order_w])
+    st = learned.stats()
+    assert st["proposal_cells"] > 0
+    assert st["proposal_second_step"] <= int(sel.sum())
+    for x in (one, two, learned):
         x.close()
+
+
+@pytest.mark.parametrize("kind", ["lognormal", "protein"])
+def test_trained_network_lowers_the_expected_work(P, model, kind):
+    """What the trained network gains, on a cloud it was not trained on: the expected work per
+    cell (neighbour insertions, failed checks, second searches and validation passes, in insertion
+    units) of its proposals against the method without it (every cell checked at 16, the plain
+    form) and against an untrained network."""
+    import apo_b200
+    from apo_b200 import generators as g
+    sites = (g.lognormal_cloud(80000, 400.0 * (80000 / 5e6) ** (1 / 3), seed=51) if kind == "lognormal"
+             else g.protein_chains(160, 500, 0.01, seed=52))
+    f, _, ck = P.training_pairs(sites)
+    trained = P.expected_cost(model.ranks(f), ck).mean()
+    plain = P.expected_cost(np.full(ck.shape, P.K), ck).mean()
+    rough = P.Model.initial(f, seed=99)
+    untrained = P.expected_cost(rough.ranks(f), ck).mean()
+    print(f"{kind}: expected work per cell: trained {trained:.1f}, plain {plain:.1f}, untrained {untrained:.1f}")
+    assert trained < plain
+    assert trained < untrained
