@@ -110,6 +110,7 @@ SIGNATURES = {
     "apo2_proposal_gradients": (_I, [_P, _P, _P, _P, _U32, _P, _P]),
     "apo2_proposal_train": (_I, [_P, _P, _U64, _U32, _U32, ctypes.c_float, _U64, _P, _P, _P]),
     "apo2_set_proposal": (_I, [_P, _P]),
+    "apo2_set_precision": (_I, [_P, _U32]),
     "apo2_batch_create": (_I, [_U32, _U32, _P, _P]),
     "apo2_batch_build": (_I, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "apo2_batch_destroy": (_I, [_P]),
@@ -231,6 +232,10 @@ class AlgorithmGPU:
         APO2_ERR_CAPACITY or APO2_ERR_ITER_LIMIT still leaves the diagram readable, as the
         reference leaves it."""
         _check(self._lib.apo2_build(self._h, ctypes.c_void_p(stream), 1 if synchronize else 0))
+
+    def set_precision(self, precision: str) -> None:
+        """"fp64" (plain) or "fp32" (the FP32-filtered form) for the next builds."""
+        _check(self._lib.apo2_set_precision(self._h, {"fp64": APO2_PRECISION_FP64, "fp32": APO2_PRECISION_FP32_FILTER}[precision]))
 
     def build_and_extract(self, stream: int = 0) -> None:
         _check(self._lib.apo2_build_and_extract(self._h, ctypes.c_void_p(stream)))

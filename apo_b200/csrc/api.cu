@@ -1359,6 +1359,17 @@ apo2_status apo2_kernel_profile( apo2_handle * h, char * json, uint64_t capacity
     return APO2_OK;
 }
 
+apo2_status apo2_set_precision( apo2_handle * h, uint32_t precision )
+{
+    if ( !h || precision > APO2_PRECISION_FP32_FILTER )
+        return fail( APO2_ERR_INVALID_ARG, "invalid argument to apo2_set_precision" );
+    APO2_CUDA( cudaSetDevice( h->device ), "cudaSetDevice" );
+    APO2_CUDA( cudaDeviceSynchronize(), "set precision" ); // no build may still run with the old one
+    h->options.precision = precision;
+    h->cells.fp32        = precision == APO2_PRECISION_FP32_FILTER ? 1u : 0u;
+    return APO2_OK;
+}
+
 apo2_status apo2_set_proposal( apo2_handle * h, const apo2_proposal * model )
 {
     if ( !h || ( model && ( model->struct_size != sizeof( apo2_proposal ) || model->version != 1 ) ) )

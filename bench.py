@@ -40,7 +40,7 @@ if ROOT not in sys.path:
 
 METRIC = "sites/sec full diagram (learned-k+FP32 vs plain) at identical topology, 1 B200"
 # forms of the build the line can time (the headline is --form)
-FORMS = ("plain", "learned")
+FORMS = ("plain", "fp32", "learned", "learned_fp32")
 UNIT = "sites/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
@@ -405,7 +405,8 @@ def run_ours(args, world, rank, local):
     model = proposal.Model.load()
 
     def use_form(algo, form):
-        proposal.attach(algo, model if form == "learned" else None)
+        proposal.attach(algo, model if form.startswith("learned") else None)
+        algo.set_precision("fp32" if form.endswith("fp32") else "fp64")
 
     # --- device-resident builds (value): the headline form, then the plain form on the same handle ---
     # --shard: one diagram split over the ranks (each builds one Morton range of cells)
@@ -433,11 +434,14 @@ def run_ours(args, world, rank, local):
                     "p99_rel": float(np.percentile(errs, 99)) if errs.size else 0.0,
                     "oracle": "Newton-refined IEEE double solve of each vertex's four sites"}
 
-    forms = {args.form: {"sites_per_s": value, "ms_per_step": ms_max, "steps": args.steps,
-                         "knn_insertions": int(stats["knn_insertions"]),
-                         "proposal_cells": int(stats["proposal_cells"]),
-                         "proposal_fallbacks": int(stats["proposal_fallbacks"]),
-                         "proposal_skipped": int(stats["proposal_skipped"])}}
+    def form_stats(st):
+        return {"knn_insertions": int(st["knn_insertions"]), "certified_after_knn": int(st["certified_after_knn"]),
+                "proposal_cells": int(st["proposal_cells"]), "proposal_fallbacks": int(st["proposal_fallbacks"]),
+                "proposal_skipped": int(st["proposal_skipped"]), "second_step_cells": int(st["proposal_second_step"]),
+                "filter_tests": int(st["filter_tests"]), "filter_escalations": int(st["filter_escalations"]),
+                "validation_rounds": int(st["validation_rounds"])}
+
+    forms = {args.form: {"sites_per_s": value, "ms_per_step": ms_max, "steps": args.steps, **form_stats(stats)}}
     for other in FORMS:
         if other == args.form:
             continue
@@ -448,14 +452,13 @@ def run_ours(args, world, rank, local):
         ms2 = time_builds(algo, k2, world, stream)
         v2, ms2_max = (shard_rate if args.shard else aggregate_rate)(n, ms2, world, device)
         st2 = algo.stats()
-        forms[other] = {"sites_per_s": v2, "ms_per_step": ms2_max, "steps": k2,
-                        "knn_insertions": int(st2["knn_insertions"]),
-                        "identical_output": output_digest(algo) == digest}
+        forms[other] = {"sites_per_s": v2, "ms_per_step": ms2_max, "steps": k2, **form_stats(st2),
+                        "same_output_as_headline": output_digest(algo) == digest}
     use_form(algo, args.form)
-    learned = forms.get("learned", {})
-    if learned.get("proposal_cells"):
-        learned["fallback_rate"] = learned["proposal_fallbacks"] / learned["proposal_cells"]
-        learned["insertions_saved"] = learned["proposal_skipped"] / max(1, learned["knn_insertions"] + learned["proposal_skipped"])
+    for name in ("learned", "learned_fp32"):
+        learned = forms.get(name, {})
+        if learned.get("proposal_cells"):
+            learned["fallback_rate"] = learned["proposal_fallbacks"] / learned["proposal_cells"]
 
     # --- per-kernel times of one more build (events around every launch) ---
     prof_algo = apo_b200.AlgorithmGPU(sites, device=local, stage_timing=True, shard=shard)
@@ -547,8 +550,10 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "strong" if args.shard else "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
-        "form": {"plain": "plain (FP64 solves, K = 16)",
-                 "learned": "learned k-proposal (FP64 solves; no FP32 filter)"}[args.form],
+        "form": {"plain": "plain (FP64, K = 16, one kNN step)",
+                 "fp32": "FP32 static filter on the conflict predicates (FP64 solves)",
+                 "learned": "learned k-proposal (FP64)",
+                 "learned_fp32": "learned k-proposal + FP32 static filter"}[args.form],
         "forms": forms,
         "speedup_vs_plain": (value / plain["sites_per_s"]) if plain.get("sites_per_s") and args.form != "plain" else None,
         "run": {"parallelism": f"shards{world}" if args.shard else f"replicas{world}",
@@ -568,8 +573,9 @@ def run_once(args, local):
     from apo_b200 import proposal
     sites, _ = workload(args.workload, args.sites)
     algo = apo_b200.AlgorithmGPU(sites, device=local)
-    if args.form == "learned":
+    if args.form.startswith("learned"):
         proposal.attach(algo, proposal.Model.load())
+    algo.set_precision("fp32" if args.form.endswith("fp32") else "fp64")
     for _ in range(2):
         algo.build_and_extract(0)
         algo.output_counts()
@@ -798,7 +804,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="lognormal5m")
-    ap.add_argument("--form", default="learned", choices=FORMS, help="headline form of `value`")
+    ap.add_argument("--form", default="learned_fp32", choices=FORMS, help="headline form of `value`")
     ap.add_argument("--sites", type=int, default=None)
     ap.add_argument("--cpu-sample", type=int, default=30000, help="sites of the CPU baseline leg")
     ap.add_argument("--ref-sample", type=int, default=15000, help="sites per step of the reference arm")

@@ -249,6 +249,9 @@ typedef struct apo2_proposal
     uint16_t w3[ APO2_PROPOSAL_HIDDEN ];
 } apo2_proposal;
 
+/* Switches the precision form of a handle's next builds (apo2_options.precision). */
+apo2_status apo2_set_precision( apo2_handle * h, uint32_t precision );
+
 /* Features of every site of a built handle, in sorted (Morton) order as apo2_debug_array:
  * host float[16 * n]. */
 apo2_status apo2_proposal_features( apo2_handle * h, float * features );
