@@ -228,10 +228,14 @@ namespace apo2
         uint32_t * heavy_count  = nullptr;
         uint32_t * heavy_next   = nullptr;
         uint32_t   heavy_cap    = 0;
-        uint2 *    sub          = nullptr; // (heavy item, BVH node) subtrees of long searches
+        uint2 *    sub          = nullptr; // (search, BVH node) subtrees of long searches; the search is a
+                                           // split set-up slot (high bit set) or a heavy item
         uint32_t * sub_count    = nullptr;
         uint32_t * sub_next     = nullptr;
         uint32_t   sub_cap      = 0;
+        void *     splits       = nullptr; // set-up of each split search, computed once for its subtrees
+        uint32_t * split_count  = nullptr;
+        uint32_t   split_cap    = 0;
     };
     size_t spec_bytes( uint32_t n );
     // interval certificate of output points (certify.cu): flags (optional) and a count of the

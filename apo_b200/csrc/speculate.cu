@@ -26,6 +26,7 @@ namespace apo2
     constexpr uint32_t kHeavyBlock    = 128;
     constexpr uint32_t kHeavyStack    = 3072; // shared node stack per warp of the cooperative walk
     constexpr uint32_t kSplitAt       = 192;  // pending subtrees at which a long walk is handed out
+    constexpr uint32_t kSplitSlot     = 0x80000000u; // marks a subtree whose search set-up is cached
 #ifndef APO2_SPEC_REFILL_AT
 #define APO2_SPEC_REFILL_AT 24
 #endif
@@ -549,15 +550,23 @@ namespace apo2
             const uint32_t end = cooperative_walk( c, s, st, size, kSplitAt );
             if ( end == kWalkSplit )
             {
-                // hand the pending subtrees to other warps
-                uint32_t base = 0;
+                // hand the pending subtrees to other warps, with the search's set-up computed once
+                // for all of them (a full slot table leaves them to recompute it)
+                uint32_t base = 0, slot = 0;
                 if ( lane == 0 )
+                {
                     base = atomicAdd( b.sub_count, size );
+                    slot = atomicAdd( b.split_count, 1u );
+                    if ( slot < b.split_cap )
+                        static_cast<EdgeSearch *>( b.splits )[ slot ] = s;
+                }
                 base = __shfl_sync( 0xffffffffu, base, 0 );
+                slot = __shfl_sync( 0xffffffffu, slot, 0 );
+                const uint32_t search = slot < b.split_cap ? ( slot | kSplitSlot ) : item;
                 if ( base + size <= b.sub_cap )
                 {
                     for ( uint32_t q = lane; q < size; q += 32 )
-                        b.sub[ base + q ] = make_uint2( item, st[ q ] );
+                        b.sub[ base + q ] = make_uint2( search, st[ q ] );
                 }
                 else if ( lane == 0 )
                     send_to_exact( b, s.t, s.e );
@@ -583,8 +592,17 @@ namespace apo2
             q = __shfl_sync( 0xffffffffu, q, 0 );
             if ( q >= count )
                 break;
-            const uint2 sub = b.sub[ q ];
-            const uint2 h   = b.heavy[ sub.x ];
+            const uint2 sub    = b.sub[ q ];
+            const bool  cached = ( sub.x & kSplitSlot ) != 0;
+            EdgeSearch  s;
+            uint2       h;
+            if ( cached )
+            {
+                s = static_cast<const EdgeSearch *>( b.splits )[ sub.x & ~kSplitSlot ];
+                h = make_uint2( s.t, s.e );
+            }
+            else
+                h = b.heavy[ sub.x ];
             // another part of this edge's search already found a contributor
             if ( ( b.cell_flag[ h.x ] & kFlagOverflow )
                  || ( ( b.maybe_bits[ size_t( h.x ) * kMaybeWords + ( h.y >> 5 ) ] >> ( h.y & 31 ) ) & 1u ) )
@@ -593,8 +611,8 @@ namespace apo2
                     atomicOr( &b.maybe_bits[ size_t( h.x ) * kMaybeWords + ( h.y >> 5 ) ], 1u << ( h.y & 31 ) );
                 continue;
             }
-            EdgeSearch s;
-            search_of_heavy( c, tasks, b, h, s );
+            if ( !cached )
+                search_of_heavy( c, tasks, b, h, s );
             uint32_t size = 1;
             if ( lane == 0 )
                 st[ 0 ] = sub.y;
@@ -646,13 +664,16 @@ namespace apo2
     // long lane searches per round: log-normal radii reach 1.5 per site
     static size_t heavy_capacity( uint32_t n ) { return 6 * size_t( n ) + 65536; }
     static size_t sub_capacity( uint32_t n ) { return 4 * size_t( n ) + 65536; }
+    // searches split into subtrees per round (each hands out up to kSplitAt subtrees)
+    static size_t split_capacity( uint32_t n ) { return size_t( n ) / 8 + 4096; }
 
     size_t spec_bytes( uint32_t n )
     {
         auto a = []( size_t x ) { return ( x + 255 ) & ~size_t( 255 ); };
         return a( 4 * size_t( n ) * kNbrCap ) + a( 4 * size_t( n ) ) * 4 + a( 4 * size_t( n ) ) + a( 16 ) * 3
                + a( 4 * output_scan_scratch_words( n ) ) + a( sizeof( uint2 ) * heavy_capacity( n ) ) + a( 16 ) * 2
-               + a( 4 * size_t( n ) * kMaybeWords ) + a( sizeof( uint2 ) * sub_capacity( n ) ) + a( 16 ) * 2;
+               + a( 4 * size_t( n ) * kMaybeWords ) + a( sizeof( uint2 ) * sub_capacity( n ) ) + a( 16 ) * 2
+               + a( sizeof( EdgeSearch ) * split_capacity( n ) ) + a( 16 );
     }
 
     void spec_carve( SpecBuffers & b, void * base, uint32_t n )
@@ -693,6 +714,11 @@ namespace apo2
         b.sub_count = reinterpret_cast<uint32_t *>( p );
         p += a( 16 );
         b.sub_next  = reinterpret_cast<uint32_t *>( p );
+        p += a( 16 );
+        b.splits = p;
+        p += a( sizeof( EdgeSearch ) * split_capacity( n ) );
+        b.split_count = reinterpret_cast<uint32_t *>( p );
+        b.split_cap   = uint32_t( split_capacity( n ) );
         b.sub_cap   = uint32_t( sub_capacity( n ) );
         b.heavy_cap = uint32_t( heavy_capacity( n ) );
     }
@@ -726,6 +752,7 @@ namespace apo2
         cudaMemsetAsync( b.heavy_next, 0, sizeof( uint32_t ), s );
         cudaMemsetAsync( b.sub_count, 0, sizeof( uint32_t ), s );
         cudaMemsetAsync( b.sub_next, 0, sizeof( uint32_t ), s );
+        cudaMemsetAsync( b.split_count, 0, sizeof( uint32_t ), s );
         APO2_LAUNCH( "k_edge_speculate", s, k_edge_speculate<<<g_spec_grid, kSpecBlock, 0, s>>>( c, tasks, task_count, b, c.error ) );
         APO2_LAUNCH( "k_edge_heavy", s, k_edge_heavy<<<g_heavy_grid, kHeavyBlock, 0, s>>>( c, tasks, b, c.error ) );
         APO2_LAUNCH( "k_edge_heavy_sub", s, k_edge_heavy_sub<<<g_heavy_grid, kHeavyBlock, 0, s>>>( c, tasks, b, c.error ) );
