@@ -1189,6 +1189,15 @@ namespace apo2
                         const uint32_t j   = node - ( n - 1 );
                         bool           can = walking && node >= n - 1 && node < 2 * n - 1 && j != i && j != vx.x && j != vx.y
                                      && j != vx.z && c.status[ j ] != kBuried;
+                        // Only a leaf closer than the best so far can become the answer, so the
+                        // distance is tested first and the warp-collective neighbour scan runs
+                        // for those leaves alone (the same conjunction, fewer scans).
+                        float d = FLT_MAX;
+                        if ( can )
+                        {
+                            d   = sphere_distance( c.sites_f[ j ], fc );
+                            can = d < best;
+                        }
                         uint32_t cm = __ballot_sync( kFull, can );
                         while ( cm )
                         {
@@ -1201,12 +1210,8 @@ namespace apo2
                         }
                         if ( can )
                         {
-                            const float d = sphere_distance( c.sites_f[ j ], fc );
-                            if ( d < best )
-                            {
-                                best     = d;
-                                neighbor = j;
-                            }
+                            best     = d;
+                            neighbor = j;
                         }
                         while ( walking )
                         {
