@@ -46,11 +46,15 @@ def main():
     args = ap.parse_args()
     rng = np.random.default_rng(12345)
     feats, targets, ranks, kinds = [], [], [], []
+    skipped = 0
     t0 = time.time()
     for d in range(args.diagrams):
         kind = d % 4
         sites = site_set(kind, args.sites, int(rng.integers(1, 2**31)))
         f, y, ck = P.training_pairs(sites)
+        if f.shape[0] == 0:
+            skipped += 1
+            continue
         take = rng.permutation(f.shape[0])[: args.per_diagram]
         feats.append(f[take])
         targets.append(y[take])
@@ -74,7 +78,7 @@ def main():
     plain = P.expected_cost(np.full(held.sum(), P.K), R[held]).mean()
     learned = P.expected_cost(r, R[held]).mean()
     summary = {
-        "pairs": int(X.shape[0]), "held_out": int(held.sum()), "epochs": args.epochs, "loss": losses.tolist(),
+        "pairs": int(X.shape[0]), "diagrams_skipped_capacity": skipped, "held_out": int(held.sum()), "epochs": args.epochs, "loss": losses.tolist(),
         "margin": model.margin, "data_seconds": round(t_data, 1), "train_seconds": round(t_train, 2),
         "held_out_certified_at_proposal": float(ok.mean()),
         "held_out_second_step_share": float((r > P.K).mean()),

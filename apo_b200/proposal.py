@@ -18,7 +18,7 @@ import os
 
 import numpy as np
 
-from . import APO2_ERR_ITER_LIMIT, AlgorithmGPU, Apo2Error, _check, load_library
+from . import APO2_ERR_CAPACITY, APO2_ERR_ITER_LIMIT, AlgorithmGPU, Apo2Error, _check, load_library
 
 INPUTS, HIDDEN = 16, 64
 K = 16  # the reference's kNN list length, which the shipped model is trained for
@@ -179,7 +179,13 @@ def training_pairs(sites: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarra
         algo.build()
     except Apo2Error as e:
         # cells left uncertified after the last round are labelled like the others (the
-        # reference leaves them so too); only that status is tolerated
+        # reference leaves them so too); a set whose cells overflow the per-cell stores (the
+        # tangent-sphere lattice at some seeds, where the reference corrupts its stores) gives
+        # no pairs
+        if e.status == APO2_ERR_CAPACITY:
+            algo.close()
+            empty = np.zeros((0, INPUTS), np.float32)
+            return empty, np.zeros(0, np.float32), np.zeros(0, np.int64)
         if e.status != APO2_ERR_ITER_LIMIT:
             raise
     f = features(algo)

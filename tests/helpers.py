@@ -14,7 +14,10 @@ STORED_CASES = ["prec0", "prec1", "prec2", "prec3", "uni2k"]
 # and knnValidationStep); their "knn" golden is the first step's list, so it is compared
 # only for single-step cases.
 STEP_CASES = ["uni2k_s2", "uni2k_k4s3", "prec1_k8s0", "prec2_k1s4", "uni2k_s0"]
-DIGEST_CASES = ["uniform_small", "protein20k", "latticeA20", "uni100k", "logn50k", "protein100k"]
+DIGEST_CASES = ["uniform_small", "protein20k", "latticeA20", "uni100k", "logn50k", "protein100k",
+                # full size: the bench's 1M protein-like packing (config 1), the 50^3 tangent-sphere
+                # lattice (config 2 A) and a 500k log-normal cloud at the 5M evaluation density (config 3)
+                "protein1m", "latticeA50", "logn500k"]
 # The oracle's IEEE single-precision square root differs in the last bit from the GPU's
 # approximate one; on the protein-like packing and the jittered lattices that flips kNN
 # orders and near-threshold predicates, so the oracle is pinned on the other cases only.

@@ -35,7 +35,7 @@ def test_fp32_form_matches_reference_dump(apo, case):
     algo.close()
 
 
-@pytest.mark.parametrize("case", ["uni100k", "logn50k", "protein100k", "latticeA20"])
+@pytest.mark.parametrize("case", ["uni100k", "logn50k", "protein100k", "latticeA20", "protein1m", "logn500k"])
 def test_fp32_form_matches_reference_digests(apo, case):
     d = H.digests()[case]
     algo = apo.AlgorithmGPU(H.sites_for(case), precision="fp32")
