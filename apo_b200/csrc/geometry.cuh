@@ -111,28 +111,30 @@ namespace apo2
     // FP32 static filter of the conflict predicate intersects(site, x) above, as the reference
     // evaluates it: d = double(sqrtf(float(|c - x|^2))) - (r + w) < 1e-8, with the approximate
     // single-precision square root of --use_fast_math. The filter recomputes d from the float
-    // copy of the site in IEEE single precision (every operation rounded to nearest, u = 2^-24)
-    // and bounds its distance from the reference's value:
+    // copy of the site in single precision (products and sums rounded to nearest, u = 2^-24; the
+    // root is the same approximate one) and bounds its distance from the reference's value:
     //   the rounding of x to float and of each difference        u (|x|_1 + 1.01 |d|_1)
-    //   the dot product and the square root                        3.5 u L
-    //   the radii sum, the final difference                        u (r + 2.01 |w| + 1.01 |d32|)
-    //   the reference: float(D) and the approximate sqrt (<= 16u)  16.5 u L
-    //   a float copy of a double site                              u (|c|_1 + r)
-    // with |d|_1 <= sqrt(3) L; twice that sum (and a tiny absolute term for flushed subnormals)
-    // is the bound E. A value with d32 - E >= 1e-8 is certainly not a conflict of the reference,
-    // one with d32 + E < 1e-8 certainly is; anything in between (2) is left to the exact test.
+    //   the dot product                                          3 u L
+    //   this filter's approximate root (<= 8u relative)          8 u L
+    //   the radii sum, the final difference                      u (r + 2.01 |w| + 1.01 |d32|)
+    //   the reference: float(D) and its approximate root         16.5 u L
+    //   a float copy of a double site                            u (|c|_1 + r)
+    // with |d|_1 <= sqrt(3) L (the approximate roots are taken at four times their documented
+    // accuracy); twice that sum, plus a tiny absolute term for flushed subnormals, is the bound
+    // E. A value with d32 - E >= 1e-8 is certainly not a conflict of the reference, one with
+    // d32 + E < 1e-8 certainly is; anything in between (2) is left to the exact test.
     __device__ __forceinline__ int conflict_filter( float4 s, double4 x )
     {
         const float xx = __double2float_rn( x.x ), xy = __double2float_rn( x.y ), xz = __double2float_rn( x.z );
         const float xw = __double2float_rn( x.w );
         const float dx = __fsub_rn( s.x, xx ), dy = __fsub_rn( s.y, xy ), dz = __fsub_rn( s.z, xz );
         const float dd = __fadd_rn( __fadd_rn( __fmul_rn( dx, dx ), __fmul_rn( dy, dy ) ), __fmul_rn( dz, dz ) );
-        const float L  = __fsqrt_rn( dd );
+        const float L  = sqrtf( dd );
         const float d  = __fsub_rn( L, __fadd_rn( s.w, xw ) );
         const float mag = fabsf( xx ) + fabsf( xy ) + fabsf( xz ) + fabsf( s.x ) + fabsf( s.y ) + fabsf( s.z );
-        const float E   = 1.1920929e-7f * ( mag + 22.f * L + 2.f * fabsf( s.w ) + 2.02f * fabsf( xw ) + 1.01f * fabsf( d ) )
+        const float E   = 1.1920929e-7f * ( mag + 30.f * L + 2.f * fabsf( s.w ) + 2.02f * fabsf( xw ) + 1.01f * fabsf( d ) )
                         + 1e-18f;
-        const double dd32 = double( d ), e64 = double( E );
+        const double dd32 = double( d ), e64 = double( E ); // compared in double against the double threshold
         if ( dd32 - e64 >= 1e-8 )
             return 0;
         if ( dd32 + e64 < 1e-8 )

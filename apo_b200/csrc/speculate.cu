@@ -163,6 +163,9 @@ namespace apo2
         bool     hyperbola;
         const uint32_t * nbr;
         uint32_t nbr_count;
+        // the third sites of the edge's vertices: the neighbours bounding its arc, which a
+        // candidate root outside the arc almost always lies inside (tested first)
+        uint32_t hint[ 2 ];
     };
 
     // Bounding volume of edge (k, l) of cell i and the security-radius test
@@ -205,11 +208,19 @@ namespace apo2
         // reach of the search: largest radius over the edge's arc
         double         wmax = 0.0;
         const uint32_t vn   = c.vertex_nb[ s.i ];
+        s.hint[ 0 ] = s.hint[ 1 ] = kNone;
         for ( uint32_t v = 0; v < vn; v++ )
         {
             const uint4 r = c.vertices[ store_row( c, s.i ) * kMaxVertices + v ];
             if ( vertex_on_edge( r, s.k, s.l ) )
-                wmax = fmax( wmax, solve_vertex( c, s.si, r ).w );
+            {
+                wmax             = fmax( wmax, solve_vertex( c, s.si, r ).w );
+                const uint32_t m = ( r.x != s.k && r.x != s.l ) ? r.x : ( ( r.y != s.k && r.y != s.l ) ? r.y : r.z );
+                if ( s.hint[ 0 ] == kNone )
+                    s.hint[ 0 ] = m;
+                else if ( s.hint[ 1 ] == kNone && m != s.hint[ 0 ] )
+                    s.hint[ 1 ] = m;
+            }
         }
         if ( ellipse || s.closed )
         {
@@ -268,9 +279,18 @@ namespace apo2
             return false;
         // the FP32 filter decides here too; its counts are kept for the cell kernels only
         FilterTally untallied;
+        // A root is empty when no neighbour other than k, l conflicts with it: the neighbours
+        // bounding the edge's arc go first (a root outside the arc is nearly always inside one of
+        // them), then the whole sorted list. The conjunction is the same.
+        bool hint_ok[ 2 ] = { false, false };
+        for ( uint32_t h = 0; h < 2; h++ )
+            hint_ok[ h ] = s.hint[ h ] != kNone && in_sorted( s.nbr, s.nbr_count, s.hint[ h ] );
         for ( uint32_t r = 0; r < 2; r++ )
         {
             bool ok = true;
+            for ( uint32_t h = 0; h < 2 && ok; h++ )
+                if ( hint_ok[ h ] )
+                    ok = !site_conflict( c, s.hint[ h ], x[ r ], untallied );
             for ( uint32_t q = 0; q < s.nbr_count && ok; q++ )
             {
                 const uint32_t u = s.nbr[ q ];
