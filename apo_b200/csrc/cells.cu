@@ -1496,6 +1496,7 @@ namespace apo2
                     w.e[ e ].w = ( w.e[ e ].w & 0xffffff00u ) | 2u;
             __syncwarp();
             bool           changedCell = false;
+            bool           pristine    = true; // no update has touched the loaded cell yet
             const uint32_t steps       = w.en / 32 + 1;
             uint32_t       restarts    = 0;
             bool             monotone = proof.maybe_bits != nullptr; // neighbours still include U0
@@ -1560,6 +1561,10 @@ namespace apo2
                 // reach of the search (see reach_radius): the stored vertices and the ones
                 // added by this pass that lie on the edge, and its possible apexes
                 float4 reach = make_float4( fsi.x, fsi.y, fsi.z, 0.f );
+                // the third sites of the stored vertices on this edge: the neighbours bounding its
+                // arc, tested first against a candidate root while the cell is the stored one
+                // (whose vertex sites are all edge sites, so they belong to the same conjunction)
+                uint32_t hint0 = kNone, hint1 = kNone;
                 if ( need )
                 {
                     double         wmax = 0.0;
@@ -1568,7 +1573,14 @@ namespace apo2
                     {
                         const uint4 r = c.vertices[ store_row( c, i ) * kMaxVertices + v ];
                         if ( vertex_on_edge( r, k, l ) )
-                            wmax = fmax( wmax, solve_vertex( c, si, r ).w );
+                        {
+                            wmax             = fmax( wmax, solve_vertex( c, si, r ).w );
+                            const uint32_t m = ( r.x != k && r.x != l ) ? r.x : ( ( r.y != k && r.y != l ) ? r.y : r.z );
+                            if ( hint0 == kNone )
+                                hint0 = m;
+                            else if ( hint1 == kNone && m != hint0 )
+                                hint1 = m;
+                        }
                     }
                     for ( uint32_t v = 0; v < w.vn; v++ )
                         if ( vertex_on_edge( w.v[ v ], k, l ) )
@@ -1710,8 +1722,11 @@ namespace apo2
                         {
                             const uint32_t nv = __ffs( tm ) - 1;
                             tm &= ~( 1u << nv );
-                            const double4 cand = shfl4( nv ? x1 : x0, t2 );
-                            const bool    ok   = edges_clear( c, w, cand, tk, tl );
+                            const double4  cand = shfl4( nv ? x1 : x0, t2 );
+                            const uint32_t h0 = __shfl_sync( kFull, hint0, t2 ), h1 = __shfl_sync( kFull, hint1, t2 );
+                            const bool     hinted = pristine && ( ( h0 != kNone && site_conflict( c, h0, cand, w.tally ) )
+                                                              || ( h1 != kNone && site_conflict( c, h1, cand, w.tally ) ) );
+                            const bool     ok   = !hinted && edges_clear( c, w, cand, tk, tl );
                             if ( lane == t2 && !ok )
                                 valid &= ~( 1u << nv );
                         }
@@ -1768,6 +1783,7 @@ namespace apo2
                     if ( is_known( w, tj ) )
                         continue;
                     const bool changed = update_cell( c, w, i, si, tj, c.sites[ tj ], err );
+                    pristine           = false;
                     if ( monotone )
                     {
                         const uint32_t   cnt0 = proof.nbr_count[ slot ];

@@ -73,7 +73,7 @@ def main():
     t_train = time.time() - t1
     # margin: the worst generator's expected work relative to the plain form's, minimised, so that
     # no kind of input pays for another's gain
-    model.margin = P.choose_margin(model, X[held], R[held], groups=K[held])
+    model.margin, model.max_rank = P.choose_policy(model, X[held], R[held], groups=K[held])
     model.save(args.out)
     r = model.ranks(X[held])
     ok = (R[held] > 0) & (R[held] <= r)
@@ -89,7 +89,7 @@ def main():
                 "second_step_share": float((r[sel] > P.K).mean())}
     summary = {
         "pairs": int(X.shape[0]), "diagrams_skipped_capacity": skipped, "held_out": int(held.sum()), "epochs": args.epochs, "loss": losses.tolist(),
-        "margin": model.margin, "data_seconds": round(t_data, 1), "train_seconds": round(t_train, 2),
+        "margin": model.margin, "max_rank": model.max_rank, "data_seconds": round(t_data, 1), "train_seconds": round(t_train, 2),
         "held_out_certified_at_proposal": float(ok.mean()),
         "held_out_second_step_share": float((r > P.K).mean()),
         "held_out_expected_cost": {"plain": plain, "learned": learned, "per_generator": per_kind},

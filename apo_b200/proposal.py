@@ -217,24 +217,40 @@ def expected_cost(ranks: np.ndarray, certified_k: np.ndarray, k: int = K, valida
     return np.where(one, c1, c2)
 
 
-def choose_margin(model: Model, features: np.ndarray, certified_k: np.ndarray, k: int = K, groups=None) -> float:
-    """Margin minimising the expected work per cell (expected_cost) on held-out data. With
-    `groups` (one label per pair, e.g. the generator of its diagram) the margin minimises the worst
-    group's work relative to the plain form's, so that no kind of input is made slower to speed
-    up another."""
+def choose_policy(model: Model, features: np.ndarray, certified_k: np.ndarray, k: int = K, groups=None) -> tuple[float, int]:
+    """(margin, max_rank) minimising the expected work per cell (expected_cost) on held-out data:
+    early checks only (max_rank = k) or with the second kNN step (max_rank = 2k). With `groups`
+    (the generator of each pair's diagram) the worst group's work relative to the plain form's is
+    minimised, so that no kind of input is made slower to speed up another. A margin that sends
+    every proposal to k (no early check, no second step) is among the candidates: where nothing
+    pays, the network leaves the plain construction as it is."""
     pred = model.predict(features).astype(np.float64)
     ck = np.asarray(certified_k)
     plain = expected_cost(np.full(ck.shape, k), ck, k)
-    keys = [None] if groups is None else sorted(set(np.asarray(groups).tolist()))
-    best, best_score = 0.0, np.inf
-    for m in np.arange(-3.0, 2.01, 0.125):
-        r = np.clip(np.ceil(np.exp2(pred + m)), 1, model.max_rank)
+    g = None if groups is None else np.asarray(groups)
+    keys = None if g is None else sorted(set(g.tolist()))
+    best, best_score = (64.0, k), np.inf
+    for max_rank in (k, 2 * k):
+        for m in list(np.arange(-3.0, 2.01, 0.125)) + [64.0]:
+            r = np.clip(np.ceil(np.exp2(np.minimum(pred + m, 30.0))), 1, max_rank)
+            cost = expected_cost(r, ck, k)
+            score = cost.mean() if g is None else max(cost[g == key].mean() / plain[g == key].mean() for key in keys)
+            if score < best_score - 1e-12:
+                best, best_score = (float(m), int(max_rank)), float(score)
+    return best
+
+
+def choose_margin(model: Model, features: np.ndarray, certified_k: np.ndarray, k: int = K, groups=None) -> float:
+    """The margin of choose_policy for the model's own max_rank."""
+    pred = model.predict(features).astype(np.float64)
+    ck = np.asarray(certified_k)
+    plain = expected_cost(np.full(ck.shape, k), ck, k)
+    g = None if groups is None else np.asarray(groups)
+    best, best_score = 64.0, np.inf
+    for m in list(np.arange(-3.0, 2.01, 0.125)) + [64.0]:
+        r = np.clip(np.ceil(np.exp2(np.minimum(pred + m, 30.0))), 1, model.max_rank)
         cost = expected_cost(r, ck, k)
-        if groups is None:
-            score = cost.mean()
-        else:
-            g = np.asarray(groups)
-            score = max(cost[g == key].mean() / plain[g == key].mean() for key in keys)
-        if score < best_score:
+        score = cost.mean() if g is None else max(cost[g == key].mean() / plain[g == key].mean() for key in set(g.tolist()))
+        if score < best_score - 1e-12:
             best, best_score = float(m), float(score)
     return best

@@ -125,7 +125,7 @@ def model(P):
     ck = np.concatenate([p[2] for p in pairs])
     m = P.Model.initial(x, seed=7)
     m.train(x, y, epochs=4)
-    m.margin = P.choose_margin(m, x, ck)
+    m.margin, m.max_rank = P.choose_policy(m, x, ck)
     return m
 
 
