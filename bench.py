@@ -51,11 +51,15 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 C_QUAD = 216
 C_TEST = 11
 
-# DRAM bytes (read + write) per site of one build, by kernel, from one ncu capture of the
-# protein-like packing at 100,000 sites (--set full, one kernel per capture), scaled by the
-# sites processed.
-TRAFFIC_BYTES_PER_SITE = {"k_vertex_validation": 1839.3, "k_edge_speculate": 1536.5, "k_cells": 316.6,
-                          "k_bisector_validation": 1054.6}
+# DRAM bytes (read + write) per site of one launch, by kernel, from one-kernel ncu captures (--set
+# full, the kernel's first launch), scaled by the sites processed: the log-normal cloud of 1M sites
+# at the evaluation density for the edge-search kernels, the protein-like packing of 100,000 sites
+# for the others.
+TRAFFIC_BYTES_PER_SITE = {"k_edge_heavy_sub": (22334.4, "1M log-normal capture"),
+                          "k_edge_speculate": (1418.2, "1M log-normal capture"),
+                          "k_vertex_validation": (1839.3, "100k protein-like capture"),
+                          "k_cells": (316.6, "100k protein-like capture"),
+                          "k_bisector_validation": (1054.6, "100k protein-like capture")}
 
 
 def measure_fp64_peak(device) -> float:
@@ -493,10 +497,10 @@ def run_ours(args, world, rank, local):
     roofline = {
         "bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": achieved / peaks["hbm_gbs"],
-        "traffic": (TRAFFIC_BYTES_PER_SITE[dom_name] * n / max(1, dom_count)
-                    if dom_name in TRAFFIC_BYTES_PER_SITE else None),
-        "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch from a 100k-site protein "
-                        "capture, scaled by sites", "peak_kind": peaks_kind,
+        "traffic": (TRAFFIC_BYTES_PER_SITE[dom_name][0] * n if dom_name in TRAFFIC_BYTES_PER_SITE else None),
+        "traffic_note": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the kernel's first (largest) launch, "
+                         f"{TRAFFIC_BYTES_PER_SITE[dom_name][1]}, scaled by sites" if dom_name in TRAFFIC_BYTES_PER_SITE
+                         else "no capture of this kernel"), "peak_kind": peaks_kind,
         "kernel_share": dom_ms / total_ms, "kernel_avg_launch_ms": dom_avg_ms, "kernel_launches": dom_count,
         "algorithmic_bytes_per_diagram": b_alg,
         "note": "the path is latency-bound (dependent BVH-node and site loads in divergent walks, warp-collective "
