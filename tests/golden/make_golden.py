@@ -18,6 +18,8 @@ Usage:
     python tests/golden/make_golden.py <dump_root>    (dump_root/<case>/*.u32 ...) -> fixtures
     python tests/golden/make_golden.py outputs <dump_root> <case>   <case>_ref.npz: the reference's
         output vertices (ids and positions) of one case, e.g. latticeB20 for the arbitration test
+    python tests/golden/make_golden.py cells <dump_root> <case> <cell> ...   <case>_cells.npz: the
+        reference's store records of the listed cells (sorted index), e.g. logn500k 350405 405638
 """
 from __future__ import annotations
 
@@ -153,10 +155,27 @@ def write_outputs(root: str, case: str) -> None:
     print(case, ids.size // 4, "output vertices")
 
 
+def write_cells(root: str, case: str, cells: list[int]) -> None:
+    """The reference's store records (vertex and edge rows, 4 words each, store order) of a few
+    cells of one case, by sorted cell index: the cells where this build's stores depart from the
+    reference's (tests/test_gpu_parity.py arbitrates them)."""
+    dump = load_dump(root, case)
+    out = {"cells": np.asarray(cells, dtype=np.int64)}
+    for store, counts in (("vertices", "vertex_nb"), ("edges", "edge_nb")):
+        ends = np.cumsum(dump[counts].astype(np.int64))
+        rows = dump[store].reshape(-1, 4)
+        for i in cells:
+            out[f"{store}_{i}"] = rows[ends[i] - dump[counts][i]:ends[i]].copy()
+    np.savez_compressed(os.path.join(HERE, f"{case}_cells.npz"), **out)
+    print(case, "records of", len(cells), "cells")
+
+
 if __name__ == "__main__":
     if sys.argv[1] == "inputs":
         write_inputs(sys.argv[2], sys.argv[3:] or None)
     elif sys.argv[1] == "outputs":
         write_outputs(sys.argv[2], sys.argv[3])
+    elif sys.argv[1] == "cells":
+        write_cells(sys.argv[2], sys.argv[3], [int(x) for x in sys.argv[4:]])
     else:
         main(sys.argv[1])

@@ -84,10 +84,14 @@ def test_gpu_matches_reference_digests(apo, case):
     d = H.digests()[case]
     algo = apo.AlgorithmGPU(H.sites_for(case))
     algo.build()
+    # the cells arbitrated in test_departing_cells_hold_a_refuted_vertex carry the reference's
+    # records here; every other cell must be bit-identical
+    stores = H.stores_with_reference_cells(algo, case)
     for name in H.EXACT:
         if name.startswith("topo_"):
             continue
-        assert H.sha(algo.debug_array(name)) == d["arrays"][name], f"{case}: {name}"
+        a = stores[name] if name in stores else algo.debug_array(name)
+        assert H.sha(a) == d["arrays"][name], f"{case}: {name}"
     full = algo.toHostFull(True)
     assert H.sha(full.verticesId) == d["arrays"]["vertices_id"]
     assert H.sha(H.closed_ids3(full.closedEdgesId)) == d["arrays"]["closed_id"]
@@ -256,4 +260,62 @@ def test_topology_json_matches_topology(apo):
     assert np.array_equal(np.asarray(data["bisectors"], np.uint32).reshape(-1), golden["topo_bi"])
     assert np.array_equal(np.asarray(data["trisectors"], np.uint32).reshape(-1), golden["topo_tri"])
     assert np.array_equal(np.asarray(data["quadrisectors"], np.uint32).reshape(-1), golden["topo_quad"])
+    algo.close()
+
+
+def _vertex_roots(s1, s2, s3, s4):
+    """Both spheres tangent to four sites, (x, y, z, w) with w measured from s1, in IEEE double
+    (the algebra of the reference's vertex solve, gpu/math.cuh:703-780, without its
+    single-precision square root)."""
+    p = [np.asarray(s[:3], np.float64) for s in (s1, s2, s3, s4)]
+    r = [float(s[3]) for s in (s1, s2, s3, s4)]
+    nh = np.array([np.append(p[0] - p[q], r[0] - r[q]) for q in (1, 2, 3)])
+    mc = np.array([.5 * (-p[0] @ p[0] + p[q] @ p[q] + r[0] * r[0] - r[q] * r[q]) for q in (1, 2, 3)])
+    inv = np.linalg.inv(nh[:, :3])
+    mn, mb = -inv @ nh[:, 3], inv @ mc
+    e = -mn * r[0] - mb - p[0]
+    a, b, c = mn @ mn - 1.0, 2.0 * (mn @ e), e @ e
+    q = -.5 * (b - np.copysign(1.0, b) * np.sqrt(max(b * b - 4 * a * c, 0.0)))
+    out = []
+    for xd in (c / q - r[0], q / a - r[0]):
+        v = mn * xd - mb
+        out.append(np.append(v, np.linalg.norm(p[0] - v) - r[0]))
+    return out
+
+
+def test_departing_cells_hold_a_refuted_vertex(apo):
+    """The 500k log-normal cloud (5M-cloud density): in two cells the reference's store holds one
+    vertex more than this build's, with its two edges. Its fourth site lies 60-160 units away, and
+    its stored root lies 1e8 units from the cell's site, where the reference's distance (a double
+    squared length rounded to float before a single-precision square root) is off by ~10 units,
+    more than the 4-6 units by which the cell's own neighbours overlap that root: the
+    reference's emptiness check passes on rounding noise. This build's edge search never tests
+    the site (its contributors must lie within a ball bounded by the edge's arc). Bar: every other
+    cell bit-identical (the digest test), the departing cells' records otherwise identical, and the
+    extra vertex refuted by the interval certificate (another site certainly closer)."""
+    ref = H.reference_cells("logn500k")
+    algo = apo.AlgorithmGPU(H.sites_for("logn500k"))
+    algo.build()
+    S = algo.debug_array("sites_sorted").reshape(-1, 4)
+    idx = algo.debug_array("indices")
+    mv = H.per_cell_rows(algo.debug_array("vertices"), algo.debug_array("vertex_nb"))
+    me = H.per_cell_rows(algo.debug_array("edges"), algo.debug_array("edge_nb"))
+    for i in ref["cells"].tolist():
+        rv, re_ = ref[f"vertices_{i}"], ref[f"edges_{i}"]
+        # one vertex appended to the reference's store, the rest identical in order
+        assert rv.shape[0] == mv[i].shape[0] + 1 and np.array_equal(rv[:-1], mv[i])
+        a, b, c, flag = (int(x) for x in rv[-1])
+        known = set(me[i][:, :2].ravel().tolist())
+        j = next(x for x in (a, b, c) if x not in known)
+        k, l = (x for x in (a, b, c) if x != j)
+        # two edges appended; the edge (k, l) differs only in its status and vertex-count words
+        assert re_.shape[0] == me[i].shape[0] + 2
+        assert np.array_equal(re_[:-2, :2], me[i][:, :2])
+        same = ~((re_[:-2, 0] == min(k, l)) & (re_[:-2, 1] == max(k, l))) & ~((re_[:-2, 0] == max(k, l)) & (re_[:-2, 1] == min(k, l)))
+        assert np.array_equal(re_[:-2][same], me[i][same])
+        assert {tuple(sorted(r[:2])) for r in re_[-2:].tolist()} == {tuple(sorted((j, k))), tuple(sorted((j, l)))}
+        x = _vertex_roots(S[i], S[j], S[k], S[l])[flag & 0xff]
+        assert x[3] > 1e7
+        bad, _ = algo.certify(x, [idx[i], idx[j], idx[k], idx[l]])
+        assert bad == 1, (i, j, x)
     algo.close()

@@ -129,6 +129,17 @@ def model(P):
     return m
 
 
+@pytest.fixture(scope="module")
+def exercised(model):
+    """The model with an eager policy (proposals lowered by one rank, second searches up to rank
+    32), so that the parity test meets both early checks and second kNN steps whatever policy the
+    shipped model carries: the cells must match the reference's for every policy."""
+    import copy
+    m = copy.deepcopy(model)
+    m.margin, m.max_rank = -1.0, 32
+    return m
+
+
 def _build(apo, sites, model):
     from apo_b200 import proposal as P
     algo = apo.AlgorithmGPU(sites)
@@ -146,7 +157,7 @@ def _per_cell(algo, name, counts):
 
 
 @pytest.mark.parametrize("kind", ["lognormal", "protein"])
-def test_learned_form_builds_the_reference_cells(P, model, kind):
+def test_learned_form_builds_the_reference_cells(P, exercised, kind):
     """Every cell of the learned form ends as the reference's build leaves it with one kNN step
     (proposed rank <= 16) or two (proposed beyond 16): status, known radius, both stores record by
     record, and the output vertices the cell owns."""
@@ -158,7 +169,7 @@ def test_learned_form_builds_the_reference_cells(P, model, kind):
     one.build()
     two = apo_b200.AlgorithmGPU(sites, knnValidationStep=2)
     two.build()
-    learned = _build(apo_b200, sites, model)
+    learned = _build(apo_b200, sites, exercised)
     sel = learned.debug_array("proposed_k") > 16
     for name in ("status", "known_radii", "vertex_nb", "edge_nb"):
         want = np.where(sel, two.debug_array(name), one.debug_array(name))
@@ -186,7 +197,7 @@ def test_learned_form_builds_the_reference_cells(P, model, kind):
     assert np.array_equal(mi[order_m], wi[order_w])
     assert np.array_equal(mp[order_m], wp[order_w])
     st = learned.stats()
-    assert st["proposal_cells"] > 0
+    assert st["proposal_cells"] > 0 and sel.any()
     assert st["proposal_second_step"] <= int(sel.sum())
     for x in (one, two, learned):
         x.close()
