@@ -743,26 +743,40 @@ namespace apo2
         b.heavy_cap = uint32_t( heavy_capacity( n ) );
     }
 
-    static int g_spec_grid = 0, g_heavy_grid = 0;
+    // Persistent grid sizes per device (148 SMs x resident blocks of each kernel on B200).
+    constexpr int        kSpecDevices = 64;
+    static int           g_spec_grid[ kSpecDevices ], g_heavy_grid[ kSpecDevices ];
+    static PerDeviceOnce g_spec_config;
+
+    static int spec_device()
+    {
+        int dev = 0;
+        cudaGetDevice( &dev );
+        return ( dev >= 0 && dev < kSpecDevices ) ? dev : -1;
+    }
 
     void configure_spec_kernels()
     {
-        if ( g_spec_grid != 0 )
-            return;
-        int dev = 0, sms = 148, per_sm = 0;
-        cudaGetDevice( &dev );
-        cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_edge_speculate, kSpecBlock, 0 );
-        const int spec = sms * std::max( 1, per_sm );
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_edge_heavy, kHeavyBlock, 0 );
-        g_heavy_grid = sms * std::max( 1, per_sm );
-        g_spec_grid  = spec;
+        g_spec_config.run( [] {
+            const int dev = spec_device();
+            if ( dev < 0 )
+                return;
+            int sms = 148, per_sm = 0;
+            cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_edge_speculate, kSpecBlock, 0 );
+            g_spec_grid[ dev ] = sms * std::max( 1, per_sm );
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_edge_heavy, kHeavyBlock, 0 );
+            g_heavy_grid[ dev ] = sms * std::max( 1, per_sm );
+        } );
     }
 
     void launch_edge_validation_speculative( const CellContext & c, const uint32_t * tasks, const uint32_t * task_count,
                                              const SpecBuffers & b, cudaStream_t s )
     {
         configure_spec_kernels();
+        const int dev        = spec_device();
+        const int spec_grid  = dev >= 0 ? g_spec_grid[ dev ] : 148 * 4; // an ordinal outside the table
+        const int heavy_grid = dev >= 0 ? g_heavy_grid[ dev ] : 148 * 4;
         const uint32_t nbr_blocks = std::max( 1u, std::min<uint32_t>( ( c.n + 3 ) / 4, 148 * 32 ) );
         APO2_LAUNCH( "k_neighbor_lists", s, k_neighbor_lists<<<nbr_blocks, kNbrBlock, 0, s>>>( c, tasks, task_count, b ) );
         scan_exclusive( b.item_count, c.n, b.scan_sums, b.item_total, s );
@@ -773,9 +787,9 @@ namespace apo2
         cudaMemsetAsync( b.sub_count, 0, sizeof( uint32_t ), s );
         cudaMemsetAsync( b.sub_next, 0, sizeof( uint32_t ), s );
         cudaMemsetAsync( b.split_count, 0, sizeof( uint32_t ), s );
-        APO2_LAUNCH( "k_edge_speculate", s, k_edge_speculate<<<g_spec_grid, kSpecBlock, 0, s>>>( c, tasks, task_count, b, c.error ) );
-        APO2_LAUNCH( "k_edge_heavy", s, k_edge_heavy<<<g_heavy_grid, kHeavyBlock, 0, s>>>( c, tasks, b, c.error ) );
-        APO2_LAUNCH( "k_edge_heavy_sub", s, k_edge_heavy_sub<<<g_heavy_grid, kHeavyBlock, 0, s>>>( c, tasks, b, c.error ) );
+        APO2_LAUNCH( "k_edge_speculate", s, k_edge_speculate<<<spec_grid, kSpecBlock, 0, s>>>( c, tasks, task_count, b, c.error ) );
+        APO2_LAUNCH( "k_edge_heavy", s, k_edge_heavy<<<heavy_grid, kHeavyBlock, 0, s>>>( c, tasks, b, c.error ) );
+        APO2_LAUNCH( "k_edge_heavy_sub", s, k_edge_heavy_sub<<<heavy_grid, kHeavyBlock, 0, s>>>( c, tasks, b, c.error ) );
         APO2_LAUNCH( "k_edge_commit", s, k_edge_commit<<<std::max( 1u, std::min<uint32_t>( ( c.n + 7 ) / 8, 148 * 16 ) ), 256, 0, s>>>( c, tasks, task_count, b ) );
         SearchProof proof;
         proof.slots      = b.exact_slot;
