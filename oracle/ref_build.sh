@@ -1,9 +1,10 @@
 #!/usr/bin/env bash
 # Builds the reference apo GPU library from its own sources, exactly as its CMake target
 # compiles them (nvcc, --use_fast_math, relocatable device code, extended lambdas), for
-# sm_100a, and links it with oracle/ref_driver.cu. Two binaries come out:
+# sm_100a, and links it with oracle/ref_driver.cu. Three binaries come out:
 #   oracle/_ref/apo_ref_driver       default `apo` target (FP64 Real)
 #   oracle/_ref/apo_ref_driver_fp32  `apo-fp32` target (-DAPO_REAL_SIZE=4)
+#   oracle/_ref/apo_ref_contrib      the contributing-nearest study (oracle/ref_contrib.cu)
 # The only file not taken from the reference is oracle/ref_shim/fmt/*, a logging stub
 # for the missing `fmt` submodule. Nothing here is copied into the repository; the
 # reference sources are read where they lie. Outputs go to oracle/_ref/ only.
@@ -44,5 +45,12 @@ build() {
 }
 build apo_ref_driver &
 build apo_ref_driver_fp32 -DAPO_REAL_SIZE=4 &
+# the contributing-nearest study's labels, through oracle/ref_contrib.cu (its harness source is
+# included where it lies; its own headers under app/ are found there too)
+CONTRIB_SRC="$REF/app/benchmarks/benchmark_contributing_nearest.cu"
+if [ -f "$CONTRIB_SRC" ]; then
+    SOURCES[${#SOURCES[@]}-1]="$HERE/ref_contrib.cu"
+    build apo_ref_contrib -DAPO_CONTRIB_SOURCE="\"$CONTRIB_SRC\"" -I "$REF/app" &
+fi
 wait
 echo "reference drivers in $OUT"

@@ -1,5 +1,6 @@
-// Minimal stand-in for the two `fmt` entry points the reference's GPU library names
-// (`fmt::print` in its cudaCheck helper, `fmt::format` in its logger template).
+// Minimal stand-in for the `fmt` entry points the reference's GPU library names
+// (`fmt::print` in its cudaCheck helper, `fmt::format` in its logger template) and
+// `fmt::format_to`, which its contributing-nearest study's CSV writer names.
 // The `fmt` submodule is not vendored with the reference; this stub only formats
 // log text ("{}" placeholders, format specs ignored) and takes no part in any
 // computation. Used solely by oracle/ref_build.sh.
@@ -39,6 +40,15 @@ namespace fmt
         std::string_view   rest = pattern;
         detail::append( out, rest, args... );
         return out.str();
+    }
+
+    template<class OutputIt, class... T>
+    OutputIt format_to( OutputIt out, std::string_view pattern, const T &... args )
+    {
+        const std::string text = format( pattern, args... );
+        for ( const char ch : text )
+            *out++ = ch;
+        return out;
     }
 
     template<class... T>

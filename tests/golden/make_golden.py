@@ -18,6 +18,9 @@ Usage:
     python tests/golden/make_golden.py <dump_root>    (dump_root/<case>/*.u32 ...) -> fixtures
     python tests/golden/make_golden.py outputs <dump_root> <case>   <case>_ref.npz: the reference's
         output vertices (ids and positions) of one case, e.g. latticeB20 for the arbitration test
+    python tests/golden/make_golden.py label-inputs <dir>; oracle/_ref/apo_ref_contrib <dir>/<case>.f32 32
+        <dir>/<case> (on a GPU, each LABEL_CASES entry); python tests/golden/make_golden.py labels <dir>:
+        the reference's contributing-nearest labels of LABEL_CASES -> <case>.npz
     python tests/golden/make_golden.py cells <dump_root> <case> <cell> ...   <case>_cells.npz: the
         reference's store records of the listed cells (sorted index), e.g. logn500k 350405 405638
 """
@@ -170,11 +173,42 @@ def write_cells(root: str, case: str, cells: list[int]) -> None:
     print(case, "records of", len(cells), "cells")
 
 
+# Inputs of the contributing-nearest label fixtures (apo_ref_contrib runs on each with 32
+# considered ranks, i.e. three kNN steps of 16).
+LABEL_CASES = {
+    "labels_uniform20k": "uniform_random(20000, 127.0, 0.5, 2.0, 31)",
+    "labels_protein20k": "protein_chains(40, 500, 0.01, seed=8)",
+}
+LABEL_CONSIDERED = 32
+
+
+def write_label_inputs(out: str) -> None:
+    os.makedirs(out, exist_ok=True)
+    for case, expr in LABEL_CASES.items():
+        eval("generators." + expr).astype(np.float32).tofile(os.path.join(out, case + ".f32"))  # noqa: S307
+
+
+def write_labels(root: str) -> None:
+    """<case>.contribution.u8 / <case>.reached.u8 written by apo_ref_contrib -> <case>.npz."""
+    for case, expr in LABEL_CASES.items():
+        n = eval("generators." + expr).shape[0]  # noqa: S307
+        arrays = {}
+        for name in ("contribution", "reached"):
+            a = np.fromfile(os.path.join(root, f"{case}.{name}.u8"), dtype=np.uint8)
+            arrays[name] = a.reshape(n, -1)
+        np.savez_compressed(os.path.join(HERE, case + ".npz"), **arrays)
+        print(case, n, "sites,", arrays["contribution"].shape[1], "ranks")
+
+
 if __name__ == "__main__":
     if sys.argv[1] == "inputs":
         write_inputs(sys.argv[2], sys.argv[3:] or None)
     elif sys.argv[1] == "outputs":
         write_outputs(sys.argv[2], sys.argv[3])
+    elif sys.argv[1] == "label-inputs":
+        write_label_inputs(sys.argv[2])
+    elif sys.argv[1] == "labels":
+        write_labels(sys.argv[2])
     elif sys.argv[1] == "cells":
         write_cells(sys.argv[2], sys.argv[3], [int(x) for x in sys.argv[4:]])
     else:

@@ -32,3 +32,25 @@ def test_profile_agrees_with_the_knn_certificate(kind):
     algo.build()
     assert algo.stats()["error_flags"] == 0
     algo.close()
+
+
+@pytest.mark.parametrize("case", ["labels_uniform20k", "labels_protein20k"])
+def test_profile_matches_the_reference_study(case):
+    """The per-rank labels against the reference's own contributing-nearest study
+    (app/benchmarks/benchmark_contributing_nearest.cu:10-302, its `compute<16>` built from its
+    source by oracle/ref_build.sh into apo_ref_contrib and run on a B200 with 32 considered
+    ranks, i.e. three kNN steps): tests/golden/<case>.npz, made by tests/golden/make_golden.py
+    label-inputs / labels. Both arrays are sorted site order, 48 ranks per site."""
+    import os
+    import apo_b200
+    from apo_b200 import generators  # noqa: F401  (named by the case table)
+    from tests.golden import make_golden as MG
+    path = os.path.join(os.path.dirname(__file__), "golden", case + ".npz")
+    ref = np.load(path)
+    sites = eval("generators." + MG.LABEL_CASES[case])  # noqa: S307 - fixed table
+    algo = apo_b200.AlgorithmGPU(sites)
+    contributed, certified, _ = algo.contribution_profile(steps=MG.LABEL_CONSIDERED // 16 + 1)
+    assert contributed.shape == ref["contribution"].shape
+    assert np.array_equal(contributed, ref["contribution"]), int((contributed != ref["contribution"]).sum())
+    assert np.array_equal(certified, ref["reached"]), int((certified != ref["reached"]).sum())
+    algo.close()
