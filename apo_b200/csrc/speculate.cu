@@ -22,10 +22,19 @@ namespace apo2
     constexpr uint32_t kSpecBlock     = 128;
     constexpr uint32_t kFlagFound     = 1;
     constexpr uint32_t kFlagOverflow  = 2;
-    constexpr uint32_t kLaneBudget    = 128;  // walk steps one lane may take before the search goes to a warp
+#ifndef APO2_SPEC_LANE_BUDGET
+#define APO2_SPEC_LANE_BUDGET 256
+#endif
+#ifndef APO2_SPEC_SPLIT_AT
+#define APO2_SPEC_SPLIT_AT 192
+#endif
+#ifndef APO2_SPEC_MIN_BLOCKS
+#define APO2_SPEC_MIN_BLOCKS 4
+#endif
+    constexpr uint32_t kLaneBudget    = APO2_SPEC_LANE_BUDGET; // walk steps one lane may take before the search goes to a warp
     constexpr uint32_t kHeavyBlock    = 128;
     constexpr uint32_t kHeavyStack    = 3072; // shared node stack per warp of the cooperative walk
-    constexpr uint32_t kSplitAt       = 192;  // pending subtrees at which a long walk is handed out
+    constexpr uint32_t kSplitAt       = APO2_SPEC_SPLIT_AT; // pending subtrees at which a long walk is handed out
     constexpr uint32_t kSplitSlot     = 0x80000000u; // marks a subtree whose search set-up is cached
 #ifndef APO2_SPEC_REFILL_AT
 #define APO2_SPEC_REFILL_AT 24
@@ -303,7 +312,7 @@ namespace apo2
         return false;
     }
 
-    __global__ void __launch_bounds__( kSpecBlock, 4 ) k_edge_speculate( CellContext c, const uint32_t * __restrict__ tasks,
+    __global__ void __launch_bounds__( kSpecBlock, APO2_SPEC_MIN_BLOCKS ) k_edge_speculate( CellContext c, const uint32_t * __restrict__ tasks,
                                                                       const uint32_t * __restrict__ task_count,
                                                                       SpecBuffers b, uint32_t * error )
     {
