@@ -109,7 +109,10 @@ namespace apo2
     // search still running then is finished by the whole warp, in the same order, from a
     // frontier of at most kCoopCap nodes kept in global scratch (plus each lane's saved stack),
     // kCoopWidth x 32 frontier nodes per step.
-    constexpr uint32_t kLaneWalk         = 256;
+#ifndef APO2_EXACT_LANE_WALK
+#define APO2_EXACT_LANE_WALK 256
+#endif
+    constexpr uint32_t kLaneWalk         = APO2_EXACT_LANE_WALK;
 #ifndef APO2_COOP_WIDTH
 #define APO2_COOP_WIDTH 4
 #endif
