@@ -1326,24 +1326,30 @@ apo2_status apo2_kernel_profile( apo2_handle * h, char * json, uint64_t capacity
     if ( !h )
         return fail( APO2_ERR_INVALID_ARG, "null handle" );
     APO2_CUDA( cudaDeviceSynchronize(), "kernel profile" );
-    std::map<std::string, std::pair<uint32_t, double>> per;
+    struct PerKernel
+    {
+        uint32_t launches = 0;
+        double   total_ms = 0.0, max_ms = 0.0;
+    };
+    std::map<std::string, PerKernel> per;
     for ( const auto & r : h->records )
     {
         float ms = 0.f;
         if ( r.end >= 0 )
             cudaEventElapsedTime( &ms, h->event_pool[ r.begin ], h->event_pool[ r.end ] );
         auto & x = per[ r.name ];
-        x.first++;
-        x.second += ms;
+        x.launches++;
+        x.total_ms += ms;
+        x.max_ms = std::max( x.max_ms, double( ms ) );
     }
     std::string out = "{\"launches\": " + std::to_string( h->launches ) + ", \"timed\": " + ( h->timing ? "true" : "false" )
                       + ", \"kernels\": {";
     bool first = true;
     for ( const auto & kv : per )
     {
-        char buf[ 160 ];
-        std::snprintf( buf, sizeof( buf ), "%s\"%s\": [%u, %.6f]", first ? "" : ", ", kv.first.c_str(), kv.second.first,
-                       kv.second.second );
+        char buf[ 192 ];
+        std::snprintf( buf, sizeof( buf ), "%s\"%s\": [%u, %.6f, %.6f]", first ? "" : ", ", kv.first.c_str(),
+                       kv.second.launches, kv.second.total_ms, kv.second.max_ms );
         out += buf;
         first = false;
     }

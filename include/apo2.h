@@ -351,7 +351,7 @@ apo2_status apo2_debug_array( apo2_handle * h, const char * name, void * dst, ui
 apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats );
 
 /* Kernel launches of the last build as JSON text: {"launches": L, "timed": bool, "kernels":
- * {"name": [count, total_ms], ...}} (times only with stage_timing). With json == NULL only
+ * {"name": [count, total_ms, longest_launch_ms], ...}} (times only with stage_timing). With json == NULL only
  * *length is set. */
 apo2_status apo2_kernel_profile( apo2_handle * h, char * json, uint64_t capacity, uint64_t * length );
 
