@@ -211,7 +211,7 @@ apo2_status apo2_topology_json( apo2_handle * h, char * json, uint64_t capacity,
 apo2_status apo2_certify( apo2_handle * h, const double * positions, const uint32_t * ids, uint64_t count, uint32_t arity,
                           apo2_location location, uint8_t * flags, uint64_t * bad );
 
-/* Learned k-proposal (the north star's learned form; the reference only measures the labels,
+/* Learned k-proposal (a per-cell kNN rank chosen by a network; the reference only measures the labels,
  * app/benchmarks/benchmark_contributing_nearest.cu:10-129). A 16 -> 64 -> 64 -> 1 network with
  * ReLU, bf16 weights and fp32 accumulation predicts log2 of the kNN rank at which a site's cell
  * passes the security-radius certificate, from 16 features of the site (radius, Morton-local

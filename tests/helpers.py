@@ -30,7 +30,7 @@ EXACT = ["indices", "parent", "left", "right", "aabb", "sizes", "sites_sorted", 
 # Vertex positions of the CPU oracle against the reference: the oracle evaluates double
 # arithmetic without fused multiply-adds and single-precision square roots with IEEE sqrtf
 # (the reference uses the approximate hardware root), so positions agree to this relative
-# tolerance (the north-star bound is 1e-5 relative).
+# tolerance (the positional bound the path is held to is 1e-5 relative).
 ORACLE_POSITION_RTOL = 1e-5
 
 
