@@ -95,7 +95,7 @@ namespace apo2
     }
 
 #ifndef APO2_LANE_CLEAR_EDGES
-#define APO2_LANE_CLEAR_EDGES 16
+#define APO2_LANE_CLEAR_EDGES 8
 #endif
     // cells with at most this many edges check new roots lane by lane in update_cell
     constexpr uint32_t kLaneClearEdges = APO2_LANE_CLEAR_EDGES;
