@@ -377,7 +377,8 @@ class AlgorithmGPU:
         return out
 
     def kernel_profile(self) -> dict:
-        """Kernels of the last build: launch count and, with stage_timing, per-kernel times."""
+        """Kernels of the last build: {"launches", "timed", "kernels": {name: [count, total_ms,
+        longest_launch_ms]}} (times only with stage_timing)."""
         import json
         length = ctypes.c_uint64()
         _check(self._lib.apo2_kernel_profile(self._h, None, 0, ctypes.byref(length)))
