@@ -212,6 +212,9 @@ namespace
     apo2_status enqueue_build( apo2_handle * h, cudaStream_t s )
     {
         const uint32_t n = h->n;
+        // the error check below is about this build's launches: an error another call left
+        // behind (not one that broke the context, which every call reports again) is dropped
+        cudaGetLastError();
         ObserveScope   observe( h );
         h->launches    = 0;
         h->events_used = 0;
@@ -1304,11 +1307,18 @@ apo2_status apo2_get_stats( apo2_handle * h, apo2_stats * stats )
     s.proposal_second_step = cnt[ kCountSecondStep ];
     s.filter_escalations = cnt[ kCountEscalated ];
     s.kernel_launches = h->launches;
-    if ( h->timing )
+    if ( h->timing && h->built )
     {
-        float ms[ kStages ] = {};
-        for ( int e = 0; e < 7; e++ )
-            cudaEventElapsedTime( &ms[ e ], h->events[ e ], h->events[ e + 1 ] );
+        // the output span's closing event is recorded by an extraction only; an elapsed time
+        // asked of an unrecorded event would fail and leave a stale error behind
+        float      ms[ kStages ] = {};
+        const int  spans         = h->extracted ? 7 : 6;
+        for ( int e = 0; e < spans; e++ )
+            if ( cudaEventElapsedTime( &ms[ e ], h->events[ e ], h->events[ e + 1 ] ) != cudaSuccess )
+            {
+                ms[ e ] = 0.f;
+                cudaGetLastError();
+            }
         s.ms_bounds              = ms[ 0 ];
         s.ms_tree                = ms[ 1 ];
         s.ms_knn                 = ms[ 2 ];
@@ -1335,8 +1345,11 @@ apo2_status apo2_kernel_profile( apo2_handle * h, char * json, uint64_t capacity
     for ( const auto & r : h->records )
     {
         float ms = 0.f;
-        if ( r.end >= 0 )
-            cudaEventElapsedTime( &ms, h->event_pool[ r.begin ], h->event_pool[ r.end ] );
+        if ( r.end >= 0 && cudaEventElapsedTime( &ms, h->event_pool[ r.begin ], h->event_pool[ r.end ] ) != cudaSuccess )
+        {
+            ms = 0.f;
+            cudaGetLastError();
+        }
         auto & x = per[ r.name ];
         x.launches++;
         x.total_ms += ms;

@@ -73,3 +73,24 @@ def test_iteration_limit_is_reported_and_the_diagram_kept(apo):
     assert lib.apo2_build(short.handle, None, 0) == apo.APO2_OK
     short.close()
     full.close()
+
+
+def test_stage_times_of_a_build_without_extraction_leave_no_error(apo):
+    """With stage timing on, the stats of a build that was not extracted have no output span
+    (its closing event is recorded by an extraction); reading them must leave no CUDA error
+    behind for the next build to report (a later handle's build once failed with
+    "invalid resource handle" that way)."""
+    from apo_b200 import generators as g
+    sites = g.uniform_random(5000, 60.0, 0.5, 2.0, 17)
+    a = apo.AlgorithmGPU(sites, stage_timing=True)
+    a.build()
+    st = a.stats()
+    assert st["ms_output"] == 0.0 and st["ms_cells"] > 0.0
+    prof = a.kernel_profile()
+    assert prof["timed"] and all(len(v) == 3 and v[2] <= v[1] + 1e-6 for v in prof["kernels"].values())
+    a.close()
+    b = apo.AlgorithmGPU(sites, stage_timing=True)
+    b.build()
+    b.build_and_extract()
+    assert b.stats()["ms_output"] >= 0.0
+    b.close()
