@@ -134,10 +134,11 @@ namespace apo2
         const float mag = fabsf( xx ) + fabsf( xy ) + fabsf( xz ) + fabsf( s.x ) + fabsf( s.y ) + fabsf( s.z );
         const float E   = 1.1920929e-7f * ( mag + 30.f * L + 2.f * fabsf( s.w ) + 2.02f * fabsf( xw ) + 1.01f * fabsf( d ) )
                         + 1e-18f;
-        const double dd32 = double( d ), e64 = double( E ); // compared in double against the double threshold
-        if ( dd32 - e64 >= 1e-8 )
+        // d - E and d + E rounded outward, against the floats just above and just below the
+        // double threshold 1e-8 (0x322bcc78 = 1.00000008e-8, 0x322bcc77 = 0.99999999e-8)
+        if ( __fsub_rd( d, E ) >= __uint_as_float( 0x322bcc78u ) )
             return 0;
-        if ( dd32 + e64 < 1e-8 )
+        if ( __fadd_ru( d, E ) < __uint_as_float( 0x322bcc77u ) )
             return 1;
         return 2;
     }
