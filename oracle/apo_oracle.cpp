@@ -448,6 +448,10 @@ namespace
         double                rmax = 0.0;
         int                   round = 0;
         uint32_t              flagsAll = 0;
+        // contributing-nearest study (app/benchmarks/benchmark_contributing_nearest.cu): per
+        // cell, knnSteps * k rank labels of the kNN cell construction
+        bool                  profile = false;
+        std::vector<uint8_t>  contribution, reached;
 
         Box box( uint32_t node ) const
         {
@@ -1188,6 +1192,40 @@ namespace
         ctx.knownRadii[ i ] = float( knownRadius );
     }
 
+    // getCellsContribution (app/benchmarks/benchmark_contributing_nearest.cu:10-129): the kNN
+    // cell construction of one step, labelling every rank with whether its neighbour changed the
+    // cell and whether the security-radius certificate held after it; the known radius starts
+    // over at every step, and a certified cell stops there.
+    void cellContribution( Context & ctx, uint32_t i, uint32_t step )
+    {
+        if ( ctx.status[ i ] == kFullyValidated || ctx.status[ i ] == kBuried )
+            return;
+        CellWork          w { ctx, i, ctx.sites[ i ], ctx.cells[ i ], ctx.flags[ i ] };
+        double            knownRadius = -DBL_MAX;
+        const std::size_t row         = std::size_t( i ) * ctx.knnSteps * ctx.k + std::size_t( ctx.k ) * step;
+        for ( uint32_t nId = 0; nId < ctx.k; nId++ )
+        {
+            const uint32_t j = ctx.knn[ std::size_t( i ) * ctx.k + nId ];
+            if ( j == kNone )
+                break;
+            if ( ctx.status[ j ] == kBuried )
+                continue;
+            const D4   sj          = ctx.sites[ j ];
+            const bool contributed = w.update( j, sj );
+            knownRadius            = dmax( knownRadius, sphereDistance( w.si, sj ) );
+            if ( contributed )
+                ctx.contribution[ row + nId ] = 1;
+            const bool over = greaterThan( knownRadius, 2.0 * w.radius() );
+            if ( over )
+            {
+                ctx.reached[ row + nId ] = 1;
+                ctx.status[ i ]          = kFullyValidated;
+                break;
+            }
+        }
+        ctx.knownRadii[ i ] = float( knownRadius );
+    }
+
     // globalVertexValidation (algorithm.inl:208-476)
     void vertexValidation( Context & ctx, uint32_t i )
     {
@@ -1848,12 +1886,22 @@ namespace
         ctx.knownRadii.assign( n, -FLT_MAX );
         for ( uint32_t i = 0; i < n; i++ )
             initialCell( ctx, ctx.cells[ i ] );
+        if ( ctx.profile )
+        {
+            ctx.contribution.assign( std::size_t( n ) * ctx.knnSteps * ctx.k, 0 );
+            ctx.reached.assign( std::size_t( n ) * ctx.knnSteps * ctx.k, 0 );
+        }
         for ( uint32_t step = 0; step < ctx.knnSteps; step++ )
         {
             if ( step > 0 )
                 parallelFor( n, threads, [ & ]( uint32_t id ) { knnSite( ctx, id, step ); } );
-            parallelFor( n, threads, [ & ]( uint32_t i ) { cellFromKnn( ctx, i ); } );
+            if ( ctx.profile )
+                parallelFor( n, threads, [ & ]( uint32_t i ) { cellContribution( ctx, i, step ); } );
+            else
+                parallelFor( n, threads, [ & ]( uint32_t i ) { cellFromKnn( ctx, i ); } );
         }
+        if ( ctx.profile )
+            return;
 
         if ( lastStage >= ORACLE_STAGE_VALIDATION )
         {
@@ -1986,7 +2034,7 @@ struct oracle_run
 namespace
 {
     oracle_run * buildFrom( std::vector<D4> && input, uint32_t n, int lastStage, int threads, uint32_t k = kK,
-                            uint32_t knnSteps = 1 )
+                            uint32_t knnSteps = 1, bool profile = false )
     {
         if ( n < 2 || k < 1 || k > kK )
             return nullptr;
@@ -2000,6 +2048,7 @@ namespace
         r->ctx.n        = n;
         r->ctx.k        = k;
         r->ctx.knnSteps = knnSteps;
+        r->ctx.profile  = profile;
         run( r->ctx, input, lastStage, threads );
         return r;
     }
@@ -2043,6 +2092,16 @@ oracle_run * oracle_build_ex( const void * sites, int is_f64, uint32_t n, uint32
     return buildFrom( std::move( input ), n, lastStage, threads, k, knn_steps );
 }
 
+oracle_run * oracle_contribution_profile( const float * sites, uint32_t n, uint32_t steps, int threads )
+{
+    if ( steps < 1 )
+        return nullptr;
+    std::vector<D4> input( n );
+    for ( uint32_t i = 0; i < n; i++ )
+        input[ i ] = { sites[ 4 * i ], sites[ 4 * i + 1 ], sites[ 4 * i + 2 ], sites[ 4 * i + 3 ] };
+    return buildFrom( std::move( input ), n, ORACLE_STAGE_CELLS, threads, kK, steps, true );
+}
+
 uint64_t oracle_get( const oracle_run * r, const char * name, const void ** data )
 {
     const Context & c = r->ctx;
@@ -2076,6 +2135,8 @@ uint64_t oracle_get( const oracle_run * r, const char * name, const void ** data
     ORACLE_ARRAY( "topo_bi", c.topoBi )
     ORACLE_ARRAY( "counters", c.counters )
     ORACLE_ARRAY( "edge_search_log", c.edgeSearchLog )
+    ORACLE_ARRAY( "contribution", c.contribution )
+    ORACLE_ARRAY( "reached", c.reached )
 #undef ORACLE_ARRAY
     if ( key == "sites_sorted" )
     {

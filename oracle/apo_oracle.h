@@ -53,10 +53,15 @@ oracle_run * oracle_build_f64( const double * sites_xyzr, uint32_t n, int last_s
 oracle_run * oracle_build_ex( const void * sites_xyzr, int is_f64, uint32_t n, uint32_t k, uint32_t knn_steps,
                               int last_stage, int threads );
 
+/* The contributing-nearest study (app/benchmarks/benchmark_contributing_nearest.cu:10-302) on
+ * float32 sites: `steps` kNN steps of 16 neighbours, each followed by the labelling kNN cell
+ * construction. Arrays "contribution" and "reached": steps * 16 bytes per site, sorted order. */
+oracle_run * oracle_contribution_profile( const float * sites_xyzr, uint32_t n, uint32_t steps, int threads );
+
 /* Looks up one result array by name; returns its element count (0 if absent) and its
  * address in *data. Names: indices parent left right aabb sizes morton sites_sorted
  * status knn known_radii vertex_nb edge_nb vertices edges out_vertices out_vertices_id
- * out_closed out_closed_id topo_quad topo_tri topo_bi. */
+ * out_closed out_closed_id topo_quad topo_tri topo_bi (contribution reached of a profile). */
 uint64_t oracle_get( const oracle_run * run, const char * name, const void ** data );
 
 /* Bit set of capacity overflows met while building (1: vertex store, 2: edge store,

@@ -97,6 +97,32 @@ def build(sites: np.ndarray, stage: int = STAGE_OUTPUT, threads: int = 0, k: int
         lib.oracle_free(handle)
 
 
+def contribution_profile(sites: np.ndarray, steps: int = 3, threads: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's contributing-nearest study (app/benchmarks/benchmark_contributing_nearest.cu:
+    10-302) on float32 (n, 4) sites: (contribution, reached) uint8 arrays of shape (n, steps * 16),
+    sorted site order."""
+    lib = _load()
+    if not getattr(lib, "_profile_ready", False):
+        lib.oracle_contribution_profile.restype = ctypes.c_void_p
+        lib.oracle_contribution_profile.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int]
+        lib._profile_ready = True
+    sites = np.ascontiguousarray(sites, dtype=np.float32)
+    n = sites.shape[0]
+    handle = lib.oracle_contribution_profile(sites.ctypes.data, n, steps, threads)
+    if not handle:
+        raise ValueError("oracle rejected the input")
+    try:
+        out = []
+        for name in ("contribution", "reached"):
+            ptr = ctypes.c_void_p()
+            count = lib.oracle_get(handle, name.encode(), ctypes.byref(ptr))
+            buf = (ctypes.c_char * count).from_address(ptr.value)
+            out.append(np.frombuffer(bytes(buf), dtype=np.uint8).reshape(n, steps * 16).copy())
+        return out[0], out[1]
+    finally:
+        lib.oracle_free(handle)
+
+
 def _load_cavity():
     lib = _load()
     if not getattr(lib, "_cavity_ready", False):
