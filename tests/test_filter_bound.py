@@ -12,6 +12,7 @@ Measured margin: on these cases the decisions stay sound with E shrunk to a quar
 and fail at an eighth, and a bound 100 times too small fails tens of thousands of them.
 """
 import numpy as np
+import pytest
 
 F = np.float32
 U_ROOT = 2.0 ** -21  # 4 ulps of a float in [1, 2): the approximate root's allowance here
@@ -59,8 +60,9 @@ def reference_range(c, x):
     return root * (1.0 - U_ROOT) - rw, root * (1.0 + U_ROOT) - rw
 
 
-def _cases(rng, m, span, wmax):
-    """Spheres x and float sites c whose reference distance sits near the 1e-8 threshold."""
+def _cases(rng, m, span, wmax, float_sites=True):
+    """Spheres x and sites c whose reference distance sits near the 1e-8 threshold (float
+    sites, as the input; or double ones, as the six bounding sites, rounded for the filter)."""
     x = np.empty((m, 4))
     x[:, :3] = rng.uniform(-span, span, (m, 3))
     x[:, 3] = rng.uniform(0.0, wmax, m) * rng.choice([1.0, 1e-3], m)
@@ -72,15 +74,17 @@ def _cases(rng, m, span, wmax):
     c = np.empty((m, 4))
     c[:, :3] = x[:, :3] + u * (r + x[:, 3] + offset)[:, None]
     c[:, 3] = r
-    c = c.astype(F).astype(np.float64)  # sites are float input
+    if float_sites:
+        c = c.astype(F).astype(np.float64)
     return c, x
 
 
-def test_filter_decisions_hold_for_every_admissible_reference_value():
+@pytest.mark.parametrize("float_sites", [True, False])
+def test_filter_decisions_hold_for_every_admissible_reference_value(float_sites):
     rng = np.random.default_rng(2024)
     decided = total = 0
     for span, wmax in ((10.0, 5.0), (500.0, 50.0), (5000.0, 500.0), (2.0e4, 5.0e3)):
-        c, x = _cases(rng, 400_000, span, wmax)
+        c, x = _cases(rng, 400_000, span, wmax, float_sites)
         f = conflict_filter(c.astype(F), x)
         dmin, dmax = reference_range(c, x)
         # "no conflict" must hold for the smallest reference value, "conflict" for the largest
